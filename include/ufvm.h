@@ -1,0 +1,188 @@
+/* ufvm.h -- C ABI of libufvm.so, the CUDA (sm_100a) implementation of uFVM's steady
+ * SIMPLE hot path: Gauss gradients, face-loop momentum assembly, Rhie-Chow face mass
+ * flux, pressure-correction assembly, the agglomeration-AMG solve with ILU / Gauss-Seidel
+ * smoothers, and the field corrections.
+ *
+ * Each entry point names the uFVM function (en9apr/Matlab_uFVM, uFVM/src/...) whose
+ * behaviour it reproduces. uFVM binds functions by MATLAB path and keeps state in the
+ * global `Domain` struct; here the state is an opaque, device-resident case handle.
+ *
+ * Conventions: plain C types only; indices are 0-based (MATLAB's are 1-based); host
+ * pointers unless a parameter is documented as a device pointer; every function returns
+ * a ufvm_status and, on error, ufvm_last_error() gives the message (the analogue of the
+ * reference's error('...') strings). One GPU, one host thread per case handle.
+ */
+#ifndef UFVM_H
+#define UFVM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  UFVM_OK = 0,
+  UFVM_E_INVALID = 1,         /* bad argument / unknown field name */
+  UFVM_E_CUDA = 2,            /* CUDA runtime error (message in ufvm_last_error) */
+  UFVM_E_OOM = 3,             /* device allocation failed */
+  UFVM_E_NAN = 4,             /* NaN residual: cfdRunCase.m:124-127 "Divergence detected!" */
+  UFVM_E_ZERO_DIAG = 5,       /* ac == 0: cfdComputeNormalizedResidual.m:77-81 */
+  UFVM_E_BC_UNSUPPORTED = 6,  /* BC combination the reference does not implement */
+  UFVM_E_AMG_LEVELS = 7,      /* W/F cycle needs >= 4 levels: cfdApplyWCycle.m indexes level 0 */
+  UFVM_E_TIMEOUT = 8,         /* a bounded device-side wait gave up */
+  UFVM_E_NOT_CONVERGED = 9    /* ufvm_run_case reached max_iter */
+} ufvm_status;
+
+/* physical patch types (constant/polyMesh/boundary) */
+enum { UFVM_PATCH_WALL = 0, UFVM_PATCH_INLET = 1, UFVM_PATCH_OUTLET = 2, UFVM_PATCH_SYMMETRY = 3,
+       UFVM_PATCH_EMPTY = 4 };
+/* boundary-condition types (0/U, 0/p boundaryField) */
+enum { UFVM_BC_FIXED_VALUE = 0, UFVM_BC_ZERO_GRADIENT = 1, UFVM_BC_NOSLIP = 2, UFVM_BC_SLIP = 3,
+       UFVM_BC_EMPTY = 4, UFVM_BC_SYMMETRY = 5 };
+/* smoothers: 'ILU' (DILU), 'SOR' (symmetric Gauss-Seidel, natural order), multicolour GS */
+enum { UFVM_SMOOTHER_ILU = 0, UFVM_SMOOTHER_SOR = 1, UFVM_SMOOTHER_MCGS = 2 };
+enum { UFVM_CYCLE_V = 0, UFVM_CYCLE_W = 1, UFVM_CYCLE_F = 2 };
+enum { UFVM_EQ_U = 0, UFVM_EQ_P = 1 };
+/* arithmetic of the pressure-correction AMG */
+enum { UFVM_PREC_FP64 = 0, UFVM_PREC_FP32_AMG = 1 };
+
+/* Reference-defect toggles: bit set = reproduce the reference, bit clear = repaired. */
+#define UFVM_Q1_VEC_BOUNDARY_COMPONENT (1 << 0)  /* cfdComputeGradientGauss0.m:57,62 */
+#define UFVM_Q2_STRESS_NOT_TRANSPOSED  (1 << 1)  /* cfdAssembleExplicitStressTerm.m:15-22 */
+#define UFVM_Q3_NOSLIP_GAMMA_TWICE     (1 << 2)  /* cfdAssembleDiffusionTerm.m:535-551, cfdGetUCoef.m:41-44 */
+#define UFVM_Q4_GRAD_WEIGHTS_SWAPPED   (1 << 3)  /* cfdInterpolateGradientsFromElementsToInteriorFaces.m:25-27 */
+#define UFVM_Q5_ROUGH_CENTRE           (1 << 4)  /* cfdProcessOpenFoamMesh.m:70-71 */
+#define UFVM_Q6_COARSE_DPHI_KEPT       (1 << 5)  /* cfdCorrectFinerLevelSolution.m:11-14 */
+#define UFVM_Q7_ILU_SKIP_ROW           (1 << 6)  /* cfdFactorizeILU.m:21 */
+#define UFVM_Q12_OUTLET_U_FACE_ROWS    (1 << 7)  /* cfdCorrectVelocityField.m:267-269 */
+#define UFVM_Q14_NOSLIP_PATCH_SUM      (1 << 8)  /* cfdAssembleDiffusionTerm.m:535,541,547 */
+#define UFVM_Q15_NOSLIP_THIRD_SIGN     (1 << 9)  /* cfdAssembleDiffusionTerm.m:539,545,551 */
+#define UFVM_Q16_ONE_CELL_COARSEST     (1 << 10) /* cfdAgglomerate.m:14 */
+#define UFVM_QUIRKS_REFERENCE          ((1 << 11) - 1)
+
+/* Raw OpenFOAM polyMesh (what cfdReadPolyMesh.m:17-214 reads), 0-based, host memory. */
+typedef struct {
+  int32_t n_points;
+  const double* points;        /* [n_points][3] */
+  int32_t n_faces;
+  const int32_t* face_start;   /* [n_faces + 1] offsets into face_nodes */
+  const int32_t* face_nodes;
+  int32_t n_interior;
+  const int32_t* owner;        /* [n_faces] */
+  const int32_t* neighbour;    /* [n_interior] */
+  int32_t n_patches;
+  const int32_t* patch_type;   /* UFVM_PATCH_* */
+  const int32_t* patch_start;
+  const int32_t* patch_n;
+} ufvm_mesh_desc;
+
+/* Settings read by uFVM from system/fvSolution, transportProperties and run.m
+ * (cfdReadSystem.m:119-252, cfdSetupAMG.m:6-20, cfdSetupSolutionMethods.m:6-14). */
+typedef struct {
+  int32_t n_correctors;        /* SIMPLE.nCorrectors */
+  int32_t fixed_element;       /* pRefCell (0-based), -1: none */
+  int32_t p_cycle;             /* UFVM_CYCLE_* */
+  int32_t p_max_cycles;        /* 30 */
+  int32_t p_max_coarse_levels; /* 10 */
+  int32_t p_pre_sweep;         /* 1 */
+  int32_t p_post_sweep;        /* 3 */
+  int32_t p_smoother;          /* UFVM_SMOOTHER_* */
+  int32_t u_smoother;          /* UFVM_SMOOTHER_* */
+  int32_t u_n_iter;            /* 10 (cfdSolver.m:12) */
+  int32_t quirks;              /* UFVM_Q* bits */
+  int32_t p_amg;               /* 1: cfdApplyAMG, 0: cfdSolver */
+  int32_t precision;           /* UFVM_PREC_* */
+  int32_t hierarchy_reuse;     /* 0: rebuild the AMG hierarchy every p solve (reference);
+                                  k > 0: rebuild the agglomeration every k solves */
+  int32_t reserved0, reserved1;
+  double nu;                   /* transportProperties nu */
+  double urf_u, urf_p;         /* relaxationFactors */
+  double tol_u, tol_p;         /* residualControl */
+  double p_termination;        /* AMG termination (rrf) 0.1 */
+  double u_rrf;                /* 0.1 */
+  double false_dt;             /* 1e9 (cfdSetupTime.m:37) */
+} ufvm_settings;
+
+typedef struct ufvm_case ufvm_case;
+
+/* Creates a device-resident case: processes the mesh on the GPU
+ * (cfdProcessOpenFoamMesh.m:15-243), sets boundary values and initial fields
+ * (cfdInitializeCase.m:14-83, cfdInitializeMdotField.m:72-86).
+ * bc_type_*: per patch UFVM_BC_*; bc_val_u [n_bfaces][3], bc_val_p [n_bfaces];
+ * U0 [n_cells][3], p0 [n_cells], mdot0 [n_faces] may be NULL (zero / computed). */
+int ufvm_case_create(const ufvm_mesh_desc* mesh, const ufvm_settings* settings,
+                     const int32_t* bc_type_u, const int32_t* bc_type_p,
+                     const double* bc_val_u, const double* bc_val_p,
+                     const double* U0, const double* p0, const double* mdot0,
+                     ufvm_case** out);
+int ufvm_case_destroy(ufvm_case* c);
+/* sizes[0..3] = n_cells, n_faces, n_interior, nnz (2 * n_interior) */
+int ufvm_case_sizes(const ufvm_case* c, int64_t* sizes);
+
+/* cfdUpdateFields (update/cfdUpdateFields.m:17-27). */
+int ufvm_update_fields(ufvm_case* c);
+/* [rms, max] = cfdAssembleEquation(name, iComponent) (assemble/cfdAssembleEquation.m:1);
+ * eq = UFVM_EQ_U (comp 0..2) or UFVM_EQ_P. */
+int ufvm_assemble_equation(ufvm_case* c, int eq, int comp, double* rms, double* max);
+/* [r0, r1] = cfdSolveEquation(name) (solve/cfdSolveEquation.m:1). */
+int ufvm_solve_equation(ufvm_case* c, int eq, double* r0, double* r1);
+/* cfdCorrectEquation(name, iComponent) (solve/correct/cfdCorrectEquation.m:1). */
+int ufvm_correct_equation(ufvm_case* c, int eq, int comp);
+/* One steady iteration of cfdRunCase (top/cfdRunCase.m:92-142). res[16]: rms U1 U2 U3 p,
+ * max (4), linear-solver initial (4), final (4). Returns UFVM_OK, UFVM_E_NAN, ... and sets
+ * *converged per cfdCheckConvergence.m:3-20. */
+int ufvm_simple_iteration(ufvm_case* c, double* res, int* converged);
+/* cfdRunCase: iterate until converged or max_iter. */
+int ufvm_run_case(ufvm_case* c, int max_iter, int* iterations, double* res);
+
+/* Field access (host copies). Names: U (3 x rows), gradU (9 x rows), p, gradp (3 x rows),
+ * PP, gradPP, DU (3 x rows), mdot (n_faces), gammaU, fluxC1, fluxC2, ac, bc, anb, dphi,
+ * scaleU. n = number of doubles in the buffer; the call fails if it is too small. */
+int ufvm_get_field(ufvm_case* c, const char* name, double* host, int64_t n, int64_t* written);
+int ufvm_set_field(ufvm_case* c, const char* name, const double* host, int64_t n);
+/* Processed geometry (same names as the theMesh struct): Sf centroid_f area CN eCN gDiff T gf
+ * walldist volume centroid_c (vectors as [n][3]). */
+int ufvm_get_geometry(ufvm_case* c, const char* name, double* host, int64_t n);
+/* AMG hierarchy of the last p solve: number of levels, per-level sizes and the
+ * cell-to-coarse maps (cfdAgglomerateLevel.m `parents`, 0-based). */
+int ufvm_get_levels(ufvm_case* c, int* n_levels, int64_t* sizes, int max_levels);
+int ufvm_get_level_array(ufvm_case* c, int level, const char* name, void* host, int64_t n,
+                         int64_t* written);  /* parents rowptr col ac anb color (int32 / double) */
+
+/* ---- stand-alone matrix kernels on DEVICE pointers (cconn-ordered CSR: row i holds the
+ * coefficients anb{i} of setup/cfdSetupCoefficients.m in cconn{i} order) ---- */
+/* r = cfdComputeResidualsArray(coefficients) (compute/cfdComputeResidualsArray.m:9-17) */
+int ufvm_compute_residuals_array(int32_t n, const int32_t* rowptr, const int32_t* col,
+                                 const double* ac, const double* anb, const double* bc,
+                                 const double* dphi, double* r, void* stream);
+/* dphi = cfdSolveSOR(...) one symmetric natural-order Gauss-Seidel sweep (solve/cfdSolveSOR.m). */
+int ufvm_solve_sor(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
+                   const double* anb, const double* bc, double* dphi, void* stream);
+/* [dc] = cfdFactorizeILU and dphi = cfdSolveILU (solve/cfdFactorizeILU.m, cfdSolveILU.m). */
+int ufvm_factorize_ilu(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
+                       const double* anb, double* dc, int32_t quirks, void* stream);
+int ufvm_solve_ilu(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
+                   const double* anb, const double* bc, const double* dc, double* dphi,
+                   void* stream);
+/* [r0, r1] = cfdSolveAlgebraicSystem(level, smoother, nIter, rrf) on one matrix
+ * (solve/cfdSolveAlgebraicSystem.m:11-66); r0/r1/iters are host outputs. */
+int ufvm_solve_algebraic_system(int32_t n, const int32_t* rowptr, const int32_t* col,
+                                const double* ac, const double* anb, const double* bc,
+                                double* dphi, int32_t smoother, int32_t n_iter, double rrf,
+                                int32_t quirks, double* r0, double* r1, int32_t* iters,
+                                void* stream);
+/* One level of cfdAgglomerateLevel + assembleAgglomeratedLHS (device pointers in, host
+ * count out). parents[n]; coarse rowptr[n+1], col/anb capacity rowptr[n] entries, ac[n]. */
+int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col,
+                           const double* ac, const double* anb, int32_t* parents,
+                           int32_t* c_rowptr, int32_t* c_col, double* c_ac, double* c_anb,
+                           int32_t* n_coarse, int32_t* nnz_coarse, void* stream);
+
+const char* ufvm_last_error(void);
+const char* ufvm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UFVM_H */

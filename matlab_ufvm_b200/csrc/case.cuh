@@ -1,0 +1,134 @@
+// case.cuh -- device-resident state of one steady SIMPLE case (the GPU counterpart of
+// uFVM's global `Domain` struct for this path: setup/cfdSetupDomain.m:11-63).
+#pragma once
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace ufvm {
+
+// Processed mesh in HBM, structure of arrays (x, y, z split) so that face and cell
+// passes read each component with unit-stride, 32-byte-sector-aligned accesses.
+struct DMesh {
+  int Nc = 0, F = 0, Fi = 0, Fb = 0, nnz = 0;
+  DArr<int> owner, neigh, cfStart, cfFace, rowptr, col, ownSlot, neiSlot, bPatch;
+  DArr<double> fCx, fCy, fCz, Sx, Sy, Sz, area, CNx, CNy, CNz, eCx, eCy, eCz, gDiff, Tx, Ty, Tz, gf, wd;
+  DArr<double> vol, cCx, cCy, cCz;
+};
+
+struct DPatch {
+  DArr<int> ptype, pstart, pcount, bcU, bcP;
+  DArr<double> pnsum;  // [patch][3] sum of n_c^2 over the patch
+};
+
+struct HPatch {
+  int n = 0;
+  std::vector<int> type, start, count, bcU, bcP;
+};
+
+// One AMG level (level 0 = the assembled matrix), cconn-ordered CSR.
+struct Level {
+  int n = 0, nnz = 0;
+  DArr<int> rowptr, col, parents, tpos;
+  DArr<double> ac, anb, bc, dphi, r, dc, rc;
+  // level schedules for the natural-order sweeps
+  bool sched_valid = false;
+  int nfwd = 0, nbwd = 0, maxw = 0;
+  DArr<int> lvl, fwdRows, fwdStart, bwdRows, bwdStart;
+  // multicolour ordering
+  bool color_valid = false;
+  int ncolor = 0;
+  DArr<int> color, colorRows, colorStart;
+  std::vector<int> h_colorStart;
+  // children of each coarse row of the NEXT level (restriction / Galerkin)
+  DArr<int> childStart, child;
+  // FP32 copies for the mixed-precision smoother
+  DArr<float> ac32, anb32, bc32, dphi32, r32;
+};
+
+// Scratch buffers for matrix-level work (owned by a Case or by a stand-alone call).
+struct LinCtx {
+  cudaStream_t stream = nullptr;
+  int nsm = 148;
+  DArr<double> part, red;      // reduction partials / results
+  DArr<int> iflag, iscan;      // flags / scan temporaries
+  DArr<unsigned int> bar;      // grid barrier: count, gen
+  DArr<int> berr;              // grid barrier timeout flag
+  int ensure(int n);
+  void release();
+};
+
+struct AmgSolver;
+struct Case;
+
+// Raw pointer bundles handed to kernels by value.
+struct MeshView {
+  int Nc, F, Fi, Fb, nnz;
+  const int *owner, *neigh, *cfStart, *cfFace, *rowptr, *col, *bPatch;
+  const double *Sx, *Sy, *Sz, *area, *CNx, *CNy, *CNz, *eCx, *eCy, *eCz, *gDiff, *Tx, *Ty, *Tz, *gf, *wd, *vol;
+  const int *ptype, *pstart, *pcount, *bcU, *bcP;
+  const double* pnsum;
+};
+
+struct FieldView {
+  int rowsU;
+  double *U0, *U1, *U2;
+  double* gU[9];  // gradient of U: gU[c * 3 + d] = dU_c / dx_d
+  double *p, *gp0, *gp1, *gp2, *PP, *gPP0, *gPP1, *gPP2;
+  double *DU0, *DU1, *DU2, *mdot, *fC1, *fC2;
+  const double *vU0, *vU1, *vU2, *vP;  // boundary values (per boundary face)
+};
+
+struct Case {
+  ufvm_settings S{};
+  DMesh M;
+  DPatch D;
+  HPatch P;
+  cudaStream_t stream = nullptr;
+  // host copies of the topology (setup only)
+  std::vector<int> h_cfStart, h_cfFace, h_rowptr, h_col, h_ownSlot, h_neiSlot;
+  // fields
+  int rowsU = 0, rowsUcap = 0, q12_max_row = -1;
+  DArr<double> U[3], gU[9], p, gp[3], PP, gPP[3], DU[3], mdot, fC1, fC2, vU[3], vP, tmp3;
+  double scaleU = 1.0;
+  // linear systems / hierarchy
+  std::vector<Level> lev;
+  int n_levels = 1;      // number of levels in use (coarsest = n_levels - 1)
+  int p_solves = 0;      // for hierarchy reuse
+  bool hierarchy_valid = false;
+  // scratch
+  LinCtx lin;
+  AmgSolver* amg = nullptr;
+  DArr<double> part, red;
+  DArr<int> flags;
+  int nsm = 148;
+  int last_amg_cycles = 0;
+
+  MeshView mv() const;
+  FieldView fv();
+
+  template <typename T>
+  int up(DArr<T>& a, const T* h, size_t n) {
+    UFVM_CHECK(dalloc(a, std::max<size_t>(n, 1)));
+    if (n) UFVM_CUDA(cudaMemcpyAsync(a.p, h, n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return UFVM_OK;
+  }
+
+  int build_mesh(const ufvm_mesh_desc* d);
+  int init_fields(const int32_t* bcu, const int32_t* bcp, const double* vu, const double* vp, const double* U0,
+                  const double* p0, const double* mdot0);
+  int update_fields();
+  int assemble_u(int comp, double* rms, double* mx);
+  int assemble_p(double* rms, double* mx);
+  int solve(int eq, double* r0, double* r1);
+  int correct_u(int comp);
+  int correct_p();
+  int iterate(double* res, int* converged);
+  int gradient(double* const* phi, int ncomp, double* const* grad, bool vector_field);
+  int fresh_level0();
+  ~Case();
+};
+
+}  // namespace ufvm

@@ -1,0 +1,594 @@
+// linsolve.cu -- residual, smoothers and grid transfers of uFVM's linear solve.
+//
+//   residual      compute/cfdComputeResidualsArray.m:9-17
+//   GS ('SOR')    solve/cfdSolveSOR.m:13-29   (natural order, level scheduled: identical
+//                 arithmetic to the sequential sweep because a row's lower neighbours sit in
+//                 earlier levels and its upper neighbours in later ones)
+//   DILU ('ILU')  solve/cfdFactorizeILU.m:5-47, solve/cfdSolveILU.m:18-93 (level scheduled)
+//   MCGS          multicolour symmetric GS (deterministic Jones-Plassmann colouring)
+//   smoother loop solve/cfdSolveAlgebraicSystem.m:11-66
+//   restriction   solve/AMG/cfdUpdateRHS.m:10-17, prolongation cfdCorrectFinerLevelSolution.m:11-14
+//
+// Roofline: residual / one GS half-sweep are HBM-bound; algorithmic bytes per row =
+// 8 (ac) + 8 (bc) + 8 (x) + 8 (r or x write) + 4 (rowptr) + nnz_row * (8 anb + 4 col).
+#include "linsolve.cuh"
+
+namespace ufvm {
+
+int LinCtx::ensure(int n) {
+  const int nb = nblocks(n) + 2;
+  UFVM_CHECK(dalloc(part, std::max(nb, 64) * 2));
+  UFVM_CHECK(dalloc(red, 16));
+  UFVM_CHECK(dalloc(iflag, 16));
+  UFVM_CHECK(dalloc(iscan, nblocks(n, 1024) * 2 + 64));
+  if (!bar.p) {
+    UFVM_CHECK(dalloc(bar, 2));
+    UFVM_CUDA(cudaMemsetAsync(bar.p, 0, 2 * sizeof(unsigned int), stream));
+  }
+  if (!berr.p) {
+    UFVM_CHECK(dalloc(berr, 1));
+    UFVM_CUDA(cudaMemsetAsync(berr.p, 0, sizeof(int), stream));
+  }
+  return UFVM_OK;
+}
+
+void LinCtx::release() {
+  dfree(part); dfree(red); dfree(iflag); dfree(iscan); dfree(bar); dfree(berr);
+}
+
+// ---------------------------------------------------------------- scan (exclusive, int)
+__global__ void k_scan_block(const int* __restrict__ in, int* out, int n, int* bsum) {
+  __shared__ int sh[1024];
+  const int base = blockIdx.x * 1024;
+  for (int t = threadIdx.x; t < 1024; t += blockDim.x) sh[t] = base + t < n ? in[base + t] : 0;
+  __syncthreads();
+  // Hillis-Steele on 1024 entries with 1024 threads
+  for (int o = 1; o < 1024; o <<= 1) {
+    int v = 0;
+    if (threadIdx.x >= o) v = sh[threadIdx.x - o];
+    __syncthreads();
+    sh[threadIdx.x] += v;
+    __syncthreads();
+  }
+  const int incl = sh[threadIdx.x];
+  const int x = base + threadIdx.x < n ? in[base + threadIdx.x] : 0;
+  if (base + threadIdx.x < n) out[base + threadIdx.x] = incl - x;
+  if (threadIdx.x == 1023) bsum[blockIdx.x] = incl;
+}
+
+__global__ void k_scan_add(int* out, int n, const int* __restrict__ boff) {
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += boff[blockIdx.x];
+}
+
+static int scan_rec(LinCtx& c, const int* in, int* out, int n, int* tmp, size_t tmpcap) {
+  const int nb = nblocks(n, 1024);
+  if ((size_t)(2 * nb + 2) > tmpcap) { set_error("scan scratch too small"); return UFVM_E_INVALID; }
+  int* bsum = tmp;
+  int* boff = tmp + nb;
+  k_scan_block<<<nb, 1024, 0, c.stream>>>(in, out, n, bsum);
+  UFVM_LAUNCH_CHECK();
+  if (nb == 1) return UFVM_OK;
+  UFVM_CHECK(scan_rec(c, bsum, boff, nb, tmp + 2 * nb, tmpcap - 2 * nb));
+  k_scan_add<<<nb, 1024, 0, c.stream>>>(out, n, boff);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+__global__ void k_scan_total(const int* __restrict__ in, const int* __restrict__ out, int n, int* total_slot) {
+  *total_slot = n > 0 ? out[n - 1] + in[n - 1] : 0;
+}
+
+// out has n + 1 entries; out[n] = total.
+int scan_exclusive(LinCtx& c, const int* in, int* out, int n, int* total_host) {
+  size_t need = 0;
+  for (int m = n; m > 1; m = nblocks(m, 1024)) need += 2 * (size_t)nblocks(m, 1024) + 2;
+  need += 8;
+  UFVM_CHECK(dalloc(c.iscan, std::max(need, c.iscan.n)));
+  if (n > 0) UFVM_CHECK(scan_rec(c, in, out, n, c.iscan.p, c.iscan.n));
+  k_scan_total<<<1, 1, 0, c.stream>>>(in, out, n, out + n);
+  UFVM_LAUNCH_CHECK();
+  if (total_host) {
+    UFVM_CUDA(cudaMemcpyAsync(total_host, out + n, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return UFVM_OK;
+}
+
+// ---------------------------------------------------------------- residual
+__device__ __forceinline__ double row_residual(int i, const int* __restrict__ rp, const int* __restrict__ col,
+                                               const double* __restrict__ ac, const double* __restrict__ anb,
+                                               const double* __restrict__ bc, const double* __restrict__ x) {
+  double v = bc[i] - ac[i] * x[i];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - anb[k] * x[col[k]];
+  return v;
+}
+
+__global__ void k_residual(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                           const double* __restrict__ ac, const double* __restrict__ anb,
+                           const double* __restrict__ bc, const double* __restrict__ x, double* __restrict__ r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = row_residual(i, rp, col, ac, anb, bc, x);
+}
+
+// sum_i |r_i| : block partials (stage 1)
+__global__ void k_sumabs_res(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                             const double* __restrict__ ac, const double* __restrict__ anb,
+                             const double* __restrict__ bc, const double* __restrict__ x, double* part) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = i < n ? fabs(row_residual(i, rp, col, ac, anb, bc, x)) : 0.0;
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// stage 2: fixed-order sum of the partials
+__global__ void k_sum_partials(int np, const double* __restrict__ part, double* out) {
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) v = v + part[k];
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) *out = v;
+}
+
+int residual(LinCtx& c, const Level& L, const double* x, double* r) {
+  k_residual<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.ac.p, L.anb.p, L.bc.p, x, r);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+int sum_abs_residual(LinCtx& c, const Level& L, const double* x, double* out_host) {
+  UFVM_CHECK(c.ensure(L.n));
+  const int nb = nblocks(L.n);
+  k_sumabs_res<<<nb, kBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.ac.p, L.anb.p, L.bc.p, x, c.part.p);
+  UFVM_LAUNCH_CHECK();
+  k_sum_partials<<<1, 1024, 0, c.stream>>>(nb, c.part.p, c.red.p);
+  UFVM_LAUNCH_CHECK();
+  UFVM_CUDA(cudaMemcpyAsync(out_host, c.red.p, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  return UFVM_OK;
+}
+
+// ---------------------------------------------------------------- level schedules
+// fwd: lvl[i] = 1 + max lvl[j] over lower neighbours j < i (0 if none); bwd: upper.
+template <bool FWD>
+__global__ void k_level_iter(int n, const int* __restrict__ rp, const int* __restrict__ col, int* lvl, int* changed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int m = 0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = col[k];
+    if (FWD ? (j < i) : (j > i)) m = max(m, __ldcg(lvl + j) + 1);
+  }
+  if (m != __ldcg(lvl + i)) {
+    __stcg(lvl + i, m);
+    *changed = 1;
+  }
+}
+
+__global__ void k_level_hist(int n, const int* __restrict__ lvl, int* cnt, int* maxl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  atomicAdd(cnt + lvl[i], 1);
+  atomicMax(maxl, lvl[i]);
+}
+
+__global__ void k_level_fill(int n, const int* __restrict__ lvl, int* cur, int* rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  rows[atomicAdd(cur + lvl[i], 1)] = i;
+}
+
+static int one_schedule(LinCtx& c, Level& L, bool fwd, DArr<int>& rows, DArr<int>& start, int& nlev) {
+  const int n = L.n;
+  UFVM_CHECK(dalloc(L.lvl, n));
+  UFVM_CUDA(cudaMemsetAsync(L.lvl.p, 0, n * sizeof(int), c.stream));
+  int changed = 1, iters = 0;
+  while (changed) {
+    // run a few relaxation passes between host checks
+    UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), c.stream));
+    for (int k = 0; k < 8; ++k) {
+      if (fwd) k_level_iter<true><<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, L.lvl.p, c.iflag.p);
+      else k_level_iter<false><<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, L.lvl.p, c.iflag.p);
+    }
+    UFVM_LAUNCH_CHECK();
+    UFVM_CUDA(cudaMemcpyAsync(&changed, c.iflag.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    UFVM_CUDA(cudaStreamSynchronize(c.stream));
+    iters += 8;
+    if (iters > n + 16) { set_error("level schedule did not converge"); return UFVM_E_INVALID; }
+  }
+  // counting sort of rows by level
+  DArr<int> cnt;
+  UFVM_CHECK(dalloc(cnt, n + 2));
+  UFVM_CUDA(cudaMemsetAsync(cnt.p, 0, (n + 2) * sizeof(int), c.stream));
+  UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 1, 0, sizeof(int), c.stream));
+  k_level_hist<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.lvl.p, cnt.p, c.iflag.p + 1);
+  UFVM_LAUNCH_CHECK();
+  int maxl = 0;
+  UFVM_CUDA(cudaMemcpyAsync(&maxl, c.iflag.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  nlev = maxl + 1;
+  UFVM_CHECK(dalloc(start, nlev + 1));
+  UFVM_CHECK(scan_exclusive(c, cnt.p, start.p, nlev, nullptr));
+  UFVM_CUDA(cudaMemcpyAsync(cnt.p, start.p, nlev * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  UFVM_CHECK(dalloc(rows, n));
+  k_level_fill<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.lvl.p, cnt.p, rows.p);
+  UFVM_LAUNCH_CHECK();
+  // widest level (host) to size the cooperative launch
+  std::vector<int> hs(nlev + 1);
+  UFVM_CUDA(cudaMemcpyAsync(hs.data(), start.p, (nlev + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  for (int l = 0; l < nlev; ++l) L.maxw = std::max(L.maxw, hs[l + 1] - hs[l]);
+  dfree(cnt);
+  return UFVM_OK;
+}
+
+// tpos[k]: position of the transposed entry (j, i) for entry k = (i, j).
+__global__ void k_tpos(int n, const int* __restrict__ rp, const int* __restrict__ col, int* tpos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = col[k];
+    int p = -1;
+    for (int q = rp[j]; q < rp[j + 1]; ++q)
+      if (col[q] == i) { p = q; break; }
+    tpos[k] = p;
+  }
+}
+
+int build_tpos(LinCtx& c, Level& L) {
+  UFVM_CHECK(dalloc(L.tpos, std::max(L.nnz, 1)));
+  k_tpos<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.tpos.p);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+int build_schedule(LinCtx& c, Level& L) {
+  if (L.sched_valid) return UFVM_OK;
+  UFVM_CHECK(c.ensure(L.n));
+  L.maxw = 0;
+  UFVM_CHECK(one_schedule(c, L, true, L.fwdRows, L.fwdStart, L.nfwd));
+  UFVM_CHECK(one_schedule(c, L, false, L.bwdRows, L.bwdStart, L.nbwd));
+  UFVM_CHECK(build_tpos(c, L));
+  L.sched_valid = true;
+  return UFVM_OK;
+}
+
+// ---------------------------------------------------------------- level-scheduled sweeps
+enum { OP_GS = 0, OP_ILU_FACT = 1, OP_ILU_FWD = 2, OP_ILU_BWD = 3 };
+
+struct SweepArgs {
+  int n, nlev, quirks;
+  const int *lstart, *rows, *rp, *col, *tpos;
+  const double *ac, *anb, *bc;
+  double *x, *dc, *rc;
+};
+
+// Lower neighbours of row j in increasing column order (the order in which the
+// reference's outer loop over i1 delivers them), visited by repeated minimum search.
+template <int OP>
+__device__ __forceinline__ void row_op(int i, const SweepArgs& a) {
+  const int k0 = a.rp[i], k1 = a.rp[i + 1];
+  if (OP == OP_GS) {
+    double v = a.bc[i];
+    for (int k = k0; k < k1; ++k) v = v - a.anb[k] * __ldcg(a.x + a.col[k]);
+    __stcg(a.x + i, v / a.ac[i]);
+  } else if (OP == OP_ILU_FACT) {
+    double d = a.ac[i];
+    int prev = -1;
+    while (true) {
+      int best = 0x7fffffff, bk = -1;
+      for (int k = k0; k < k1; ++k) {
+        const int j = a.col[k];
+        if (j < i && j > prev && j < best) { best = j; bk = k; }
+      }
+      if (bk < 0) break;
+      prev = best;
+      // Q7: the reference's factorisation loop skips row N-1 (1-based), i.e. row n-2
+      if ((a.quirks & UFVM_Q7_ILU_SKIP_ROW) && best == a.n - 2) continue;
+      const int tk = a.tpos[bk];  // the pattern is structurally symmetric, so tk >= 0
+      if (tk >= 0) d = d - a.anb[bk] * __ldcg(a.dc + best) * a.anb[tk];
+    }
+    __stcg(a.dc + i, 1.0 / d);
+  } else if (OP == OP_ILU_FWD) {
+    double v = __ldcg(a.rc + i);
+    int prev = -1;
+    while (true) {
+      int best = 0x7fffffff, bk = -1;
+      for (int k = k0; k < k1; ++k) {
+        const int j = a.col[k];
+        if (j < i && j > prev && j < best) { best = j; bk = k; }
+      }
+      if (bk < 0) break;
+      prev = best;
+      const double mat1 = __ldcg(a.dc + best) * __ldcg(a.rc + best);
+      const double mat2 = a.anb[bk] * mat1;
+      v = v - mat2;
+    }
+    __stcg(a.rc + i, v);
+  } else {  // OP_ILU_BWD
+    double v = __ldcg(a.rc + i);
+    if (i < a.n - 1) {
+      for (int k = k0; k < k1; ++k) {
+        const int j = a.col[k];
+        if (j > i) v = v - a.anb[k] * __ldcg(a.rc + j);
+      }
+    }
+    const double mat1 = __ldcg(a.dc + i) * v;
+    __stcg(a.rc + i, mat1);
+    a.x[i] = a.x[i] + mat1;
+  }
+}
+
+template <int OP>
+__global__ void k_sched_sweep(SweepArgs a, GridBarrier bar) {
+  unsigned int gen = grid_gen0(bar);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int L = 0; L < a.nlev; ++L) {
+    const int s = a.lstart[L], e = a.lstart[L + 1];
+    for (int idx = s + tid; idx < e; idx += nth) row_op<OP>(a.rows[idx], a);
+    if (L + 1 < a.nlev)
+      if (!grid_sync(bar, gen)) return;
+  }
+}
+
+// ILU: r = b - A x (into rc) before the triangular solves
+__global__ void k_ilu_res(int n, const int* __restrict__ rp, const int* __restrict__ col, const double* __restrict__ ac,
+                          const double* __restrict__ anb, const double* __restrict__ bc, const double* __restrict__ x,
+                          double* rc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double res = -ac[i] * x[i] + bc[i];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) res = res - anb[k] * x[col[k]];
+  rc[i] = res;
+}
+
+template <int OP>
+static int launch_sweep(LinCtx& c, Level& L, bool fwd, int quirks) {
+  SweepArgs a;
+  a.n = L.n; a.quirks = quirks;
+  a.nlev = fwd ? L.nfwd : L.nbwd;
+  a.lstart = fwd ? L.fwdStart.p : L.bwdStart.p;
+  a.rows = fwd ? L.fwdRows.p : L.bwdRows.p;
+  a.rp = L.rowptr.p; a.col = L.col.p; a.tpos = L.tpos.p;
+  a.ac = L.ac.p; a.anb = L.anb.p; a.bc = L.bc.p;
+  a.x = L.dphi.p; a.dc = L.dc.p; a.rc = L.rc.p;
+  GridBarrier gb{c.bar.p, c.bar.p + 1, c.berr.p};
+  int maxb = 0;
+  UFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, k_sched_sweep<OP>, kBlock, 0));
+  const int coop = std::max(1, maxb * c.nsm);
+  const int nb = std::max(1, std::min(coop, nblocks(L.maxw)));
+  void* args[] = {(void*)&a, (void*)&gb};
+  UFVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_sched_sweep<OP>, dim3(nb), dim3(kBlock), args, 0, c.stream));
+  return UFVM_OK;
+}
+
+static int check_barrier(LinCtx& c) {
+  int err = 0;
+  UFVM_CUDA(cudaMemcpyAsync(&err, c.berr.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  if (err) {
+    UFVM_CUDA(cudaMemsetAsync(c.berr.p, 0, sizeof(int), c.stream));
+    UFVM_CUDA(cudaMemsetAsync(c.bar.p, 0, 2 * sizeof(unsigned int), c.stream));
+    set_error("grid barrier timed out in a level-scheduled sweep");
+    return UFVM_E_TIMEOUT;
+  }
+  return UFVM_OK;
+}
+
+int gs_sweep(LinCtx& c, Level& L) {
+  UFVM_CHECK(c.ensure(L.n));
+  UFVM_CHECK(build_schedule(c, L));
+  UFVM_CHECK(launch_sweep<OP_GS>(c, L, true, 0));
+  UFVM_CHECK(launch_sweep<OP_GS>(c, L, false, 0));
+  return UFVM_OK;
+}
+
+int ilu_factor(LinCtx& c, Level& L, int quirks) {
+  UFVM_CHECK(c.ensure(L.n));
+  UFVM_CHECK(build_schedule(c, L));
+  UFVM_CHECK(dalloc(L.dc, L.n));
+  UFVM_CHECK(launch_sweep<OP_ILU_FACT>(c, L, true, quirks));
+  return UFVM_OK;
+}
+
+int ilu_sweep(LinCtx& c, Level& L) {
+  UFVM_CHECK(c.ensure(L.n));
+  UFVM_CHECK(build_schedule(c, L));
+  UFVM_CHECK(dalloc(L.rc, L.n));
+  k_ilu_res<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.ac.p, L.anb.p, L.bc.p, L.dphi.p, L.rc.p);
+  UFVM_LAUNCH_CHECK();
+  UFVM_CHECK(launch_sweep<OP_ILU_FWD>(c, L, true, 0));
+  UFVM_CHECK(launch_sweep<OP_ILU_BWD>(c, L, false, 0));
+  return UFVM_OK;
+}
+
+// ---------------------------------------------------------------- colouring + MCGS
+__device__ __forceinline__ unsigned int lowbias32(unsigned int x) {
+  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+  return x;
+}
+
+__global__ void k_color_select(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                               const int* __restrict__ color, int* sel, int* remaining) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  sel[i] = 0;
+  if (color[i] >= 0) return;
+  const unsigned int hi = lowbias32((unsigned int)i);
+  bool top = true;
+  for (int k = rp[i]; k < rp[i + 1] && top; ++k) {
+    const int j = col[k];
+    if (j == i || color[j] >= 0) continue;
+    const unsigned int hj = lowbias32((unsigned int)j);
+    if (hj > hi || (hj == hi && j > i)) top = false;
+  }
+  if (top) sel[i] = 1;
+  atomicAdd(remaining, 1);
+}
+
+__global__ void k_color_assign(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                               const int* __restrict__ sel, int* color, int* ncolor) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !sel[i]) return;
+  // smallest colour not used by an already coloured neighbour (bitmask over 64 colours,
+  // then linear probing beyond)
+  unsigned long long used = 0;
+  int cmax = -1;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int cj = color[col[k]];
+    if (cj >= 0 && cj < 64) used |= 1ull << cj;
+    cmax = max(cmax, cj);
+  }
+  int c = -1;
+  if (~used) c = __ffsll(~used) - 1;
+  if (c < 0 || c >= 64) {
+    for (c = 64;; ++c) {
+      bool hit = false;
+      for (int k = rp[i]; k < rp[i + 1] && !hit; ++k) hit = color[col[k]] == c;
+      if (!hit) break;
+    }
+  }
+  color[i] = c;
+  atomicMax(ncolor, c + 1);
+}
+
+int build_coloring(LinCtx& c, Level& L) {
+  if (L.color_valid) return UFVM_OK;
+  UFVM_CHECK(c.ensure(L.n));
+  const int n = L.n;
+  UFVM_CHECK(dalloc(L.color, n));
+  DArr<int> sel;
+  UFVM_CHECK(dalloc(sel, n));
+  UFVM_CUDA(cudaMemsetAsync(L.color.p, 0xff, n * sizeof(int), c.stream));
+  UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 2, 0, sizeof(int), c.stream));
+  // Each round colours (at least) the highest-priority uncoloured row, so n rounds bound it.
+  for (int round = 0; round <= n; ++round) {
+    UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), c.stream));
+    k_color_select<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, L.color.p, sel.p, c.iflag.p);
+    k_color_assign<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, sel.p, L.color.p, c.iflag.p + 2);
+    UFVM_LAUNCH_CHECK();
+    if ((round & 7) == 7 || round == n) {
+      int rem = 0;
+      UFVM_CUDA(cudaMemcpyAsync(&rem, c.iflag.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+      UFVM_CUDA(cudaStreamSynchronize(c.stream));
+      if (rem == 0) break;
+    }
+  }
+  int nc = 0;
+  UFVM_CUDA(cudaMemcpyAsync(&nc, c.iflag.p + 2, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  L.ncolor = nc;
+  // rows grouped by colour
+  DArr<int> cnt;
+  UFVM_CHECK(dalloc(cnt, nc + 2));
+  UFVM_CUDA(cudaMemsetAsync(cnt.p, 0, (nc + 2) * sizeof(int), c.stream));
+  UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 3, 0, sizeof(int), c.stream));
+  k_level_hist<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.color.p, cnt.p, c.iflag.p + 3);
+  UFVM_CHECK(dalloc(L.colorStart, nc + 1));
+  UFVM_CHECK(scan_exclusive(c, cnt.p, L.colorStart.p, nc, nullptr));
+  UFVM_CUDA(cudaMemcpyAsync(cnt.p, L.colorStart.p, nc * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  UFVM_CHECK(dalloc(L.colorRows, n));
+  k_level_fill<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.color.p, cnt.p, L.colorRows.p);
+  UFVM_LAUNCH_CHECK();
+  L.h_colorStart.resize(nc + 1);
+  UFVM_CUDA(cudaMemcpyAsync(L.h_colorStart.data(), L.colorStart.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                            c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  dfree(cnt); dfree(sel);
+  L.color_valid = true;
+  return UFVM_OK;
+}
+
+__global__ void k_gs_rows(int cnt, const int* __restrict__ rows, const int* __restrict__ rp, const int* __restrict__ col,
+                          const double* __restrict__ ac, const double* __restrict__ anb, const double* __restrict__ bc,
+                          double* x) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int i = rows[t];
+  double v = bc[i];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - anb[k] * x[col[k]];
+  x[i] = v / ac[i];
+}
+
+int mcgs_sweep(LinCtx& c, Level& L) {
+  UFVM_CHECK(build_coloring(c, L));
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int q = 0; q < L.ncolor; ++q) {
+      const int col_ = pass == 0 ? q : L.ncolor - 1 - q;
+      const int s = L.h_colorStart[col_], cnt = L.h_colorStart[col_ + 1] - s;
+      if (cnt <= 0) continue;
+      k_gs_rows<<<nblocks(cnt), kBlock, 0, c.stream>>>(cnt, L.colorRows.p + s, L.rowptr.p, L.col.p, L.ac.p, L.anb.p,
+                                                      L.bc.p, L.dphi.p);
+    }
+  }
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+// ---------------------------------------------------------------- smoother loop
+int solve_algebraic_system(LinCtx& c, Level& L, int smoother, int n_iter, double rrf, int quirks, double* r0out,
+                           double* r1out, int* iters) {
+  UFVM_CHECK(c.ensure(L.n));
+  double s0 = 0;
+  UFVM_CHECK(sum_abs_residual(c, L, L.dphi.p, &s0));
+  const double r0 = s0 / L.n;
+  double r1 = r0;
+  int it = 1;
+  if (smoother == UFVM_SMOOTHER_ILU) {
+    UFVM_CHECK(ilu_factor(c, L, quirks));
+    while (it <= n_iter && r1 > rrf * r0) {
+      UFVM_CHECK(ilu_sweep(c, L));
+      double s = 0;
+      UFVM_CHECK(sum_abs_residual(c, L, L.dphi.p, &s));
+      UFVM_CHECK(check_barrier(c));
+      r1 = s / L.n;
+      ++it;
+    }
+  } else {
+    while (it <= n_iter && r1 > rrf * r0) {
+      if (smoother == UFVM_SMOOTHER_SOR) UFVM_CHECK(gs_sweep(c, L));
+      else UFVM_CHECK(mcgs_sweep(c, L));
+      double s = 0;
+      UFVM_CHECK(sum_abs_residual(c, L, L.dphi.p, &s));
+      if (smoother == UFVM_SMOOTHER_SOR) UFVM_CHECK(check_barrier(c));
+      r1 = s / L.n;
+      ++it;
+    }
+  }
+  if (r0out) *r0out = r0;
+  if (r1out) *r1out = r1;
+  if (iters) *iters = it - 1;
+  return UFVM_OK;
+}
+
+// ---------------------------------------------------------------- transfers
+__global__ void k_restrict(int nc, const int* __restrict__ cs, const int* __restrict__ ch,
+                           const double* __restrict__ r, double* bcC) {
+  const int P = blockIdx.x * blockDim.x + threadIdx.x;
+  if (P >= nc) return;
+  double v = 0.0;
+  for (int q = cs[P]; q < cs[P + 1]; ++q) v = v + r[ch[q]];
+  bcC[P] = v;
+}
+
+__global__ void k_prolong(int n, const int* __restrict__ parents, const double* __restrict__ dC, double* dF) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dF[i] = dF[i] + dC[parents[i]];
+}
+
+int restrict_residual(LinCtx& c, Level& F, Level& C) {
+  UFVM_CHECK(dalloc(F.r, F.n));
+  UFVM_CHECK(residual(c, F, F.dphi.p, F.r.p));
+  k_restrict<<<nblocks(C.n), kBlock, 0, c.stream>>>(C.n, F.childStart.p, F.child.p, F.r.p, C.bc.p);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+int prolong(LinCtx& c, Level& F, const Level& C) {
+  k_prolong<<<nblocks(F.n), kBlock, 0, c.stream>>>(F.n, F.parents.p, C.dphi.p, F.dphi.p);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+}  // namespace ufvm

@@ -1,0 +1,60 @@
+"""The oracle's linear-algebra pieces against direct Python transliterations of the MATLAB
+loops (cfdSolveSOR.m, cfdFactorizeILU.m, cfdSolveILU.m, cfdAgglomerateLevel.m)."""
+import numpy as np
+import pytest
+
+from helpers import py_agglomerate, py_ilu_factor, py_ilu_solve, py_sor, random_diag_dominant
+from matlab_ufvm_b200 import case
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_sor_matches_transliteration(oracle_mod, seed):
+    rp, col, ac, anb, bc = random_diag_dominant(60, seed)
+    x0 = np.random.default_rng(seed).normal(size=60)
+    assert np.array_equal(oracle_mod.sor_sweep(rp, col, ac, anb, bc, x0), py_sor(rp, col, ac, anb, bc, x0))
+
+
+@pytest.mark.parametrize("q7", [True, False])
+def test_ilu_matches_transliteration(oracle_mod, q7):
+    rp, col, ac, anb, bc = random_diag_dominant(80, 3)
+    q = case.QUIRKS_REFERENCE if q7 else case.QUIRKS_REFERENCE & ~case.Q7_ILU_SKIP_ROW
+    dc = oracle_mod.ilu_factor(rp, col, ac, anb, q)
+    assert np.array_equal(dc, py_ilu_factor(rp, col, ac, anb, q7))
+    x0 = np.random.default_rng(5).normal(size=80)
+    assert np.array_equal(oracle_mod.ilu_sweep(rp, col, ac, anb, bc, dc, x0), py_ilu_solve(rp, col, ac, anb, bc, dc, x0))
+
+
+def _p_matrix(oracle_mod, n):
+    spec = case.cavity_case(n, nu=0.01)
+    oc = oracle_mod.OracleCase(spec)
+    oc.update_fields()
+    for c in range(3):
+        oc.assemble_u(c); oc.solve(0); oc.correct_u(c)
+    oc.assemble_p()
+    rp = oc.mesh.get("rowptr"); col = oc.mesh.get("col")
+    return rp, col, oc.get("ac"), oc.get("anb"), oc.get("bc")
+
+
+@pytest.mark.parametrize("n", [6, 20])
+def test_agglomeration_matches_transliteration(oracle_mod, n):
+    rp, col, ac, anb, bc = _p_matrix(oracle_mod, n)
+    par, crp, ccol, cac, canb = oracle_mod.agglomerate(rp, col, ac, anb)
+    ppar, npar = py_agglomerate(rp, col, anb)
+    assert np.array_equal(par, ppar)
+    assert len(cac) == npar
+
+
+def test_agglomeration_random_matrix(oracle_mod):
+    rp, col, ac, anb, bc = random_diag_dominant(300, 7, nbr=6)
+    par, *_ = oracle_mod.agglomerate(rp, col, ac, anb)
+    ppar, _ = py_agglomerate(rp, col, anb)
+    assert np.array_equal(par, ppar)
+
+
+def test_coloring_is_proper_and_deterministic(oracle_mod):
+    rp, col, *_ = random_diag_dominant(500, 11, nbr=6)
+    nc, c1 = oracle_mod.coloring(rp, col)
+    _, c2 = oracle_mod.coloring(rp, col)
+    assert np.array_equal(c1, c2) and c1.min() >= 0 and c1.max() == nc - 1
+    for i in range(len(rp) - 1):
+        assert np.all(c1[col[rp[i]:rp[i + 1]]] != c1[i])
