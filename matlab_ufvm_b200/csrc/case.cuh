@@ -79,6 +79,43 @@ struct FieldView {
   double *p, *gp0, *gp1, *gp2, *PP, *gPP0, *gPP1, *gPP2;
   double *DU0, *DU1, *DU2, *mdot, *fC1, *fC2;
   const double *vU0, *vU1, *vU2, *vP;  // boundary values (per boundary face)
+  double* tmp3;                        // [Fb][3] staging for outlet velocity rows
+};
+
+// Per-case descriptor read by the batched kernels. A stage kernel is launched over a
+// work list of (slot, block) pairs, so one launch advances every resident case; a single
+// case is a one-slot table. Per-slot scalars that kernels produce live in `scal`.
+struct SlotDesc {
+  MeshView m;
+  FieldView f;
+  double nu, urf_u, urf_p, fdt;
+  int quirks, fixed, rowsU, pad;
+  double *ac, *bc, *anb, *dphi;  // level-0 system (cconn-ordered CSR over m.rowptr / m.col)
+  double* scal;                  // SCAL_* entries below
+  int* flags;                    // FLAG_* entries below
+};
+enum { SCAL_SCALE = 0, SCAL_RMS = 1, SCAL_MAX = 2, SCAL_MINMAX = 3, SCAL_N = 8 };
+enum { FLAG_ZERO_DIAG = 0, FLAG_BAD_BC = 1, FLAG_N = 4 };
+
+// (slot, block) work lists of one case, per domain
+struct WorkLists {
+  DArr<int2> cells, faces, bfaces, urows;
+  int ncells = 0, nfaces = 0, nbfaces = 0, nurows = 0, urows_for = -1;
+  DArr<int> cstart, cend, ustart, uend;  // per slot: range of its entries in `cells` / `urows`
+};
+
+// Everything a batched stage launch needs: the slot table and the work lists.
+struct BatchLaunch {
+  const SlotDesc* slots;
+  const int2* wc; int nwc;   // cells
+  const int2* wf; int nwf;   // faces
+  const int2* wb; int nwb;   // boundary faces
+  const int2* wu; int nwu;   // rows of U (for the scale)
+  const int* cstart; const int* cend;
+  const int* ustart; const int* uend;
+  int nslots;
+  double* part;              // block partials, >= 2 * max(nwc, nwu) entries
+  cudaStream_t st;
 };
 
 struct Case {
@@ -103,11 +140,17 @@ struct Case {
   AmgSolver* amg = nullptr;
   DArr<double> part, red;
   DArr<int> flags;
+  DArr<double> scal;
+  DArr<SlotDesc> slot;   // one-entry table for this case
+  WorkLists wl;
   int nsm = 148;
   int last_amg_cycles = 0;
 
   MeshView mv() const;
   FieldView fv();
+  SlotDesc desc();
+  int sync_slot();
+  BatchLaunch batch();
 
   template <typename T>
   int up(DArr<T>& a, const T* h, size_t n) {
@@ -126,7 +169,6 @@ struct Case {
   int correct_u(int comp);
   int correct_p();
   int iterate(double* res, int* converged);
-  int gradient(double* const* phi, int ncomp, double* const* grad, bool vector_field);
   int fresh_level0();
   ~Case();
 };
