@@ -95,7 +95,9 @@ typedef struct {
   int32_t precision;           /* UFVM_PREC_* */
   int32_t hierarchy_reuse;     /* 0: rebuild the AMG hierarchy every p solve (reference);
                                   k > 0: rebuild the agglomeration every k solves */
-  int32_t reserved0, reserved1;
+  int32_t p_krylov;            /* service p solve: 0 plain iterative refinement (x += V(r));
+                                  1 flexible CG (FCG(1)) with the FP32 V-cycle as preconditioner */
+  int32_t reserved1;
   double nu;                   /* transportProperties nu */
   double urf_u, urf_p;         /* relaxationFactors */
   double tol_u, tol_p;         /* residualControl */
@@ -178,6 +180,33 @@ int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col,
                            const double* ac, const double* anb, int32_t* parents,
                            int32_t* c_rowptr, int32_t* c_col, double* c_ac, double* c_anb,
                            int32_t* n_coarse, int32_t* nnz_coarse, void* stream);
+
+/* ---- batched steady-case service (continuous batching of independent cases) ----
+ * Cases are admitted first-come first-served while the resident-cell budget allows, every
+ * resident case advances one SIMPLE iteration per ufvm_service_step in one launch per stage,
+ * and a case leaves the resident set when it converges (residualControl), fails, or reaches
+ * its iteration limit, freeing room for queued cases. The solver settings are shared by all
+ * cases of a service; nu and the boundary data are per case. Linear solves: multicolour
+ * Gauss-Seidel (FP64) for U, FP32 AMG inside FP64 iterative refinement for p (the service
+ * requires settings->precision == UFVM_PREC_FP32_AMG). Latencies are device time, summed
+ * over the steps a case was resident; queue time is reported separately. */
+typedef struct ufvm_service ufvm_service;
+int ufvm_service_create(const ufvm_settings* settings, int64_t max_resident_cells, ufvm_service** out);
+int ufvm_service_submit(ufvm_service* s, const ufvm_mesh_desc* mesh, double nu, const int32_t* bc_type_u,
+                        const int32_t* bc_type_p, const double* bc_val_u, const double* bc_val_p,
+                        int32_t max_iter, int64_t* ticket);
+int ufvm_service_step(ufvm_service* s, int32_t* n_resident, int32_t* n_queued, int64_t* n_finished_total);
+/* state: 0 queued, 1 resident, 2 converged, 3 stopped (not converged or failed; status in *status) */
+int ufvm_service_status(ufvm_service* s, int64_t ticket, int32_t* state, int32_t* status, int32_t* iterations,
+                        double* res16, double* latency_ms, double* queue_ms);
+int ufvm_service_get_field(ufvm_service* s, int64_t ticket, const char* name, double* host, int64_t n,
+                           int64_t* written);
+int ufvm_service_release(ufvm_service* s, int64_t ticket);
+/* Accumulated device time (ms) per phase -- update fields, U assembly, U solve, U correction,
+ * p assembly, AMG hierarchy builds, p solve, p correction -- then the number of U smoother
+ * sweeps, p V-cycles, steps and the service clock (ms). Writes min(n, 12) values. */
+int ufvm_service_stats(ufvm_service* s, double* out, int n);
+int ufvm_service_destroy(ufvm_service* s);
 
 const char* ufvm_last_error(void);
 const char* ufvm_version(void);

@@ -405,6 +405,7 @@ void free_level(Level& L, bool keep_matrix) {
   dfree(L.parents); dfree(L.tpos); dfree(L.r); dfree(L.dc); dfree(L.rc); dfree(L.lvl); dfree(L.fwdRows);
   dfree(L.fwdStart); dfree(L.bwdRows); dfree(L.bwdStart); dfree(L.color); dfree(L.colorRows); dfree(L.colorStart);
   dfree(L.childStart); dfree(L.child); dfree(L.ac32); dfree(L.anb32); dfree(L.bc32); dfree(L.dphi32); dfree(L.r32);
+  dfree(L.fr); dfree(L.fp); dfree(L.fq);
   L.sched_valid = false;
   L.color_valid = false;
 }

@@ -36,7 +36,7 @@ Case::~Case() {
   dfree(part); dfree(red); dfree(flags); dfree(scal); dfree(slot);
   dfree(wl.cells); dfree(wl.faces); dfree(wl.bfaces); dfree(wl.urows);
   dfree(wl.cstart); dfree(wl.cend); dfree(wl.ustart); dfree(wl.uend);
-  if (stream) cudaStreamDestroy(stream);
+  if (stream && owns_stream) cudaStreamDestroy(stream);
 }
 
 // solve/cfdSolveEquation.m:11-18
@@ -79,6 +79,32 @@ int Case::iterate(double* res, int* converged) {
   return UFVM_OK;
 }
 
+// Builds a case in place. `shared` is a stream owned by the caller (a service), or null
+// for a case that owns its own stream.
+int create_case_into(Case& C, const ufvm_mesh_desc* mesh, const ufvm_settings& settings, const int32_t* bc_type_u,
+                     const int32_t* bc_type_p, const double* bc_val_u, const double* bc_val_p, const double* U0,
+                     const double* p0, const double* mdot0, cudaStream_t shared) {
+  C.S = settings;
+  if (shared) {
+    C.stream = shared;
+    C.owns_stream = false;
+  } else if (cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    C.stream = nullptr;
+    set_error("cudaStreamCreate failed (no CUDA device?)");
+    return UFVM_E_CUDA;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&C.nsm, cudaDevAttrMultiProcessorCount, dev);
+  C.lin.stream = C.stream;
+  C.lin.nsm = C.nsm;
+  C.amg = new AmgSolver(C.lin);
+  UFVM_CHECK(C.build_mesh(mesh));
+  UFVM_CHECK(C.init_fields(bc_type_u, bc_type_p, bc_val_u, bc_val_p, U0, p0, mdot0));
+  UFVM_CHECK(C.lin.ensure(C.M.F));
+  return UFVM_OK;
+}
+
 }  // namespace ufvm
 
 using namespace ufvm;
@@ -109,25 +135,8 @@ int ufvm_case_create(const ufvm_mesh_desc* mesh, const ufvm_settings* settings, 
   }
   *out = nullptr;
   ufvm_case* h = new ufvm_case();
-  Case& C = h->c;
-  C.S = *settings;
-  int st = UFVM_OK;
-  do {
-    if (cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking) != cudaSuccess) {
-      set_error("cudaStreamCreate failed (no CUDA device?)");
-      st = UFVM_E_CUDA;
-      break;
-    }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&C.nsm, cudaDevAttrMultiProcessorCount, dev);
-    C.lin.stream = C.stream;
-    C.lin.nsm = C.nsm;
-    C.amg = new AmgSolver(C.lin);
-    if ((st = C.build_mesh(mesh)) != UFVM_OK) break;
-    if ((st = C.init_fields(bc_type_u, bc_type_p, bc_val_u, bc_val_p, U0, p0, mdot0)) != UFVM_OK) break;
-    if ((st = C.lin.ensure(C.M.F)) != UFVM_OK) break;
-  } while (0);
+  const int st = ufvm::create_case_into(h->c, mesh, *settings, bc_type_u, bc_type_p, bc_val_u, bc_val_p, U0, p0,
+                                        mdot0, nullptr);
   if (st != UFVM_OK) {
     delete h;
     return st;

@@ -46,6 +46,9 @@ struct Level {
   DArr<int> childStart, child;
   // FP32 copies for the mixed-precision smoother
   DArr<float> ac32, anb32, bc32, dphi32, r32;
+  // FP64 flexible-CG vectors of the level-0 refinement (residual, search direction, A times
+  // search direction)
+  DArr<double> fr, fp, fq;
 };
 
 // Scratch buffers for matrix-level work (owned by a Case or by a stand-alone call).
@@ -124,6 +127,7 @@ struct Case {
   DPatch D;
   HPatch P;
   cudaStream_t stream = nullptr;
+  bool owns_stream = true;
   // host copies of the topology (setup only)
   std::vector<int> h_cfStart, h_cfFace, h_rowptr, h_col, h_ownSlot, h_neiSlot;
   // fields
@@ -172,5 +176,9 @@ struct Case {
   int fresh_level0();
   ~Case();
 };
+
+int create_case_into(Case& C, const ufvm_mesh_desc* mesh, const ufvm_settings& settings, const int32_t* bc_type_u,
+                     const int32_t* bc_type_p, const double* bc_val_u, const double* bc_val_p, const double* U0,
+                     const double* p0, const double* mdot0, cudaStream_t shared);
 
 }  // namespace ufvm

@@ -1,0 +1,912 @@
+// fast.cu -- the batched steady-case service (many cases, one launch per stage).
+//
+// Linear solves (new in this build, declared deviations from the reference's sequential
+// smoothers; the SIMPLE stages themselves are the reference's, shared with the plain path):
+//   U : multicolour symmetric Gauss-Seidel in FP64 with the reference's stopping rule
+//       (solve/cfdSolveAlgebraicSystem.m:38-46: at most u_n_iter sweeps, stop once
+//       sum|r|/N <= rrf * initial), evaluated per case on the device.
+//   p : FP32 AMG V-cycles on the correction equation inside FP64 iterative refinement:
+//       r = b - A x in FP64, e ~ A^-1 r by one FP32 V-cycle (multicolour GS smoothing, FP32
+//       restriction / prolongation by the agglomeration maps, FP64 dense coarsest solve),
+//       x += e in FP64; cycles stop per case on the reference's rule (cfdApplyAMG.m:27-52:
+//       at most p_max_cycles, stop once sum|r| <= termination * initial).
+// The agglomeration maps are the reference's (exact seed agglomeration of the assembled p
+// matrix) built on a case's first p solve and reused; the Galerkin coarse operators are
+// recomputed in FP64 from the current matrix at every p solve.
+//
+// Roofline (FP32 MCGS half-sweep, per row): 4 ac + 4 bc + 4 x(r) + 4 x(w) + 4 colorRows
+// + 8 rowptr + nnz_row * (4 anb + 4 col + 4 x gather).
+#include "fast.cuh"
+
+namespace ufvm {
+
+#define LEV(l, s) levTab[(size_t)(l) * ns + (s)]
+
+// ---------------------------------------------------------------- FP64 fine-level kernels
+__global__ void k_res64_abs(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
+                            const SolveCtl* __restrict__ ctl, double* part) {
+  __shared__ double sh[32];
+  const int2 w = work[blockIdx.x];
+  const SlotDesc& S = slots[w.x];
+  const int i = w.y * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < S.m.Nc && ctl[w.x].active) {
+    const int* rp = S.m.rowptr;
+    double r = S.bc[i] - S.ac[i] * S.dphi[i];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) r = r - S.anb[k] * S.dphi[S.m.col[k]];
+    v = fabs(r);
+  }
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// r = b - A x (FP64) -> FP32 right-hand side of the correction; e = 0
+__global__ void k_res64_rhs(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                            const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double* part) {
+  __shared__ double sh[32];
+  const int2 w = work[blockIdx.x];
+  const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < S.m.Nc && ctl[w.x].active) {
+    const int* rp = S.m.rowptr;
+    double r = S.bc[i] - S.ac[i] * S.dphi[i];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) r = r - S.anb[k] * S.dphi[S.m.col[k]];
+    v = fabs(r);
+    if (A.fr) A.fr[i] = r;
+    A.bc[i] = (float)r;
+    A.x[i] = 0.0f;
+  }
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+__global__ void k_update64(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                           const int2* __restrict__ work, const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const SlotDesc& S = slots[w.x];
+  const int i = w.y * blockDim.x + threadIdx.x;
+  if (i < S.m.Nc) S.dphi[i] = S.dphi[i] + (double)LEV(0, w.x).x[i];
+}
+
+// ---------------------------------------------------------------- flexible CG on level 0
+// FCG(1) (Notay, SIAM J. Sci. Comput. 22 (2000) 1444) on the FP64 correction equation, with one
+// FP32 V-cycle z = V(r) as the (slightly non-symmetric, non-stationary) preconditioner:
+//   beta = (z, q_old) / (p_old, q_old),  p = z - beta p_old,  q = A p,
+//   alpha = (p, r) / (p, q),  x += alpha p,  r -= alpha q.
+// The p-correction matrix is symmetric positive semi-definite (face coefficients enter the
+// owner and neighbour rows alike), which is what CG needs; the stopping rule stays the
+// reference's (sum|r| against the initial sum). Dot products are per (slot, block) partials
+// summed per slot in a fixed order.
+__global__ void k_fcg_zq(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                         const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double* part) {
+  __shared__ double sh[32];
+  const int2 w = work[blockIdx.x];
+  const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < S.m.Nc && ctl[w.x].active && ctl[w.x].iters > 0) v = (double)A.x[i] * A.fq[i];
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+__global__ void k_fcg_p(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                        const int2* __restrict__ work, const SolveCtl* __restrict__ ctl,
+                        const double* __restrict__ zq, const double2* __restrict__ pqr) {
+  const int2 w = work[blockIdx.x];
+  const SolveCtl c = ctl[w.x];
+  if (!c.active) return;
+  const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  if (i >= S.m.Nc) return;
+  const double z = (double)A.x[i];
+  if (c.iters == 0) {
+    A.fp[i] = z;
+  } else {
+    const double pq = pqr[w.x].x;
+    const double beta = pq > 0.0 ? zq[w.x] / pq : 0.0;
+    A.fp[i] = z - beta * A.fp[i];
+  }
+}
+
+__global__ void k_fcg_q(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                        const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double2* part) {
+  __shared__ double sh[32];
+  const int2 w = work[blockIdx.x];
+  const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  double pq = 0.0, pr = 0.0;
+  if (i < S.m.Nc && ctl[w.x].active) {
+    const int* rp = S.m.rowptr;
+    const double pi = A.fp[i];
+    double q = S.ac[i] * pi;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) q = q + S.anb[k] * A.fp[S.m.col[k]];
+    A.fq[i] = q;
+    pq = pi * q;
+    pr = pi * A.fr[i];
+  }
+  pq = block_reduce<0>(pq, sh);
+  pr = block_reduce<0>(pr, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = make_double2(pq, pr);
+}
+
+__global__ void k_fcg_update(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                             const int2* __restrict__ work, const SolveCtl* __restrict__ ctl,
+                             const double2* __restrict__ pqr, double* part) {
+  __shared__ double sh[32];
+  const int2 w = work[blockIdx.x];
+  const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < S.m.Nc && ctl[w.x].active) {
+    const double2 d = pqr[w.x];
+    const double alpha = d.x > 0.0 ? d.y / d.x : 0.0;
+    S.dphi[i] = S.dphi[i] + alpha * A.fp[i];
+    const double r = A.fr[i] - alpha * A.fq[i];
+    A.fr[i] = r;
+    A.bc[i] = (float)r;
+    A.x[i] = 0.0f;
+    v = fabs(r);
+  }
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// FP64 multicolour GS row update on level 0 (rows of one colour)
+__global__ void k_mc64(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                       const int2* __restrict__ work, int color, const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
+  if (color >= A.ncolor) return;
+  const int s0 = A.colorStart[color], cnt = A.colorStart[color + 1] - s0;
+  const int t = w.y * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int i = A.colorRows[s0 + t];
+  const int* rp = S.m.rowptr;
+  double v = S.bc[i];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - S.anb[k] * S.dphi[S.m.col[k]];
+  S.dphi[i] = v / S.ac[i];
+}
+
+// per-slot sums of block partials (fixed order)
+__global__ void k_slot_sum(const int* __restrict__ ws, const int* __restrict__ we, const double* __restrict__ part,
+                           double* out) {
+  __shared__ double sh[32];
+  const int s = blockIdx.x;
+  double v = 0.0;
+  for (int k = ws[s] + (int)threadIdx.x; k < we[s]; k += blockDim.x) v = v + part[k];
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) out[s] = v;
+}
+
+__global__ void k_slot_sum2(const int* __restrict__ ws, const int* __restrict__ we,
+                            const double2* __restrict__ part, double2* out) {
+  __shared__ double sh[32];
+  const int s = blockIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int k = ws[s] + (int)threadIdx.x; k < we[s]; k += blockDim.x) { a = a + part[k].x; b = b + part[k].y; }
+  a = block_reduce<0>(a, sh);
+  b = block_reduce<0>(b, sh);
+  if (threadIdx.x == 0) out[s] = make_double2(a, b);
+}
+
+// stopping rule of cfdSolveAlgebraicSystem / cfdApplyAMG, per slot
+__global__ void k_ctrl(const SlotDesc* __restrict__ slots, int ns, const double* __restrict__ sums, SolveCtl* ctl,
+                       int first, int max_iter, double rrf, int divide_n, int r0_slot, int r1_slot, int* any) {
+  __shared__ int sany;
+  if (threadIdx.x == 0) sany = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+    const double v = divide_n ? sums[s] / slots[s].m.Nc : sums[s];
+    SolveCtl c = ctl[s];
+    if (first) {
+      c.r0 = v; c.r1 = v; c.iters = 0;
+      c.active = (0 < max_iter && v > rrf * v) ? 1 : 0;
+    } else if (c.active) {
+      c.r1 = v;
+      c.iters += 1;
+      c.active = (c.iters < max_iter && v > rrf * c.r0) ? 1 : 0;
+    }
+    ctl[s] = c;
+    slots[s].scal[r0_slot] = c.r0;
+    slots[s].scal[r1_slot] = c.r1;
+    if (r1_slot == SCAL_P_R1) slots[s].scal[SCAL_CYC] = c.iters;
+    if (c.active) atomicOr(&sany, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *any = sany;
+}
+
+__global__ void k_copy_scal(const SlotDesc* __restrict__ slots, int ns, int from, int to) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < ns) slots[s].scal[to] = slots[s].scal[from];
+}
+
+__global__ void k_set_active(SolveCtl* ctl, int ns) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < ns) ctl[s].active = 1;
+}
+
+// ---------------------------------------------------------------- FP32 AMG kernels
+__global__ void k_lev_to32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
+                           const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& A = LEV(l, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  A.ac[i] = (float)A.ac64[i];
+  for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) A.anb[k] = (float)A.anb64[k];
+}
+
+// Galerkin by summation from level l into level l+1 (assembleAgglomeratedLHS.m:16-30 order)
+__global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
+                             const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& F = LEV(l, w.x);
+  const LevDesc& C = LEV(l + 1, w.x);
+  const int P = w.y * blockDim.x + threadIdx.x;
+  if (P >= C.n) return;
+  const int c0 = C.rowptr[P], c1 = C.rowptr[P + 1];
+  for (int t = c0; t < c1; ++t) C.anb64[t] = 0.0;
+  double AC = 0.0;
+  for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) {
+    const int c = F.child[q];
+    AC = AC + F.ac64[c];
+    for (int k = F.rowptr[c]; k < F.rowptr[c + 1]; ++k) {
+      const int Q = F.parents[F.col[k]];
+      if (Q == P) {
+        AC = AC + F.anb64[k];
+      } else {
+        int pos = c0;
+        while (pos < c1 && C.col[pos] != Q) ++pos;
+        if (pos < c1) C.anb64[pos] = C.anb64[pos] + F.anb64[k];
+      }
+    }
+  }
+  C.ac64[P] = AC;
+}
+
+__global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work, int color,
+                       const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& A = LEV(l, w.x);
+  if (color >= A.ncolor) return;
+  const int s0 = A.colorStart[color], cnt = A.colorStart[color + 1] - s0;
+  const int t = w.y * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int i = A.colorRows[s0 + t];
+  float v = A.bc[i];
+  for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
+  A.x[i] = v / A.ac[i];
+}
+
+__global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
+                        const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& A = LEV(l, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  float v = A.bc[i] - A.ac[i] * A.x[i];
+  for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
+  A.r[i] = v;
+}
+
+__global__ void k_restrict32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
+                             const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& F = LEV(l, w.x);
+  const LevDesc& C = LEV(l + 1, w.x);
+  const int P = w.y * blockDim.x + threadIdx.x;
+  if (P >= C.n) return;
+  float v = 0.0f;
+  for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) v = v + F.r[F.child[q]];
+  C.bc[P] = v;
+  C.x[P] = 0.0f;
+}
+
+__global__ void k_prolong32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
+                            const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& F = LEV(l, w.x);
+  const LevDesc& C = LEV(l + 1, w.x);
+  const int i = w.y * blockDim.x + threadIdx.x;
+  if (i >= F.n) return;
+  F.x[i] = F.x[i] + C.x[F.parents[i]];
+}
+
+// Coarsest level of each slot (at most kDense rows): its FP64 solution operator X, with
+// x = X b, is formed once per p solve by Gauss-Jordan elimination with partial pivoting of
+// [M | I]; a pivot that vanishes (the pure-Neumann pressure operator is singular) pins that
+// unknown to zero, so X is the linear map of the pinned elimination. Every V-cycle then
+// applies X with one dense product. Coarsest levels above kDense rows (reached only when
+// max_coarse_levels stops the hierarchy early) get 40 FP64 Gauss-Seidel sweeps instead.
+constexpr int kDense = 64;
+// levels of at most this many rows are smoothed inside the per-slot CTA of k_coarse_vcycle
+constexpr int kCtaRows = 2048;
+constexpr int kDenseLd = kDense + 1;
+struct DenseFactorSmem {
+  double M[kDense][kDenseLd];
+  double X[kDense][kDenseLd];
+  double f[kDense];
+  double red[32];
+  int pinned[kDense];
+  int piv_row;
+};
+
+__global__ void __launch_bounds__(1024) k_coarse_factor(const LevDesc* __restrict__ levTab, int ns,
+                                                        const int* __restrict__ coarsest, double* cinv) {
+  extern __shared__ __align__(16) unsigned char dsm_raw[];
+  DenseFactorSmem& sm = *reinterpret_cast<DenseFactorSmem*>(dsm_raw);
+  const int s = blockIdx.x;
+  const LevDesc& A = LEV(coarsest[s], s);
+  const int n = A.n;
+  if (n > kDense) return;
+  for (int t = threadIdx.x; t < kDense * kDense; t += blockDim.x) {
+    const int i = t / kDense, j = t % kDense;
+    sm.M[i][j] = 0.0;
+    sm.X[i][j] = i == j ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    sm.M[i][i] = A.ac64[i];
+    for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) sm.M[i][A.col[k]] = A.anb64[k];
+    sm.pinned[i] = 0;
+  }
+  __syncthreads();
+  double mx = 0.0;
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) mx = fmax(mx, fabs(sm.M[t / n][t % n]));
+  const double scale = block_reduce<1>(mx, sm.red);
+  __shared__ double s_scale;
+  if (threadIdx.x == 0) s_scale = scale;
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (threadIdx.x == 0) {
+      int p = k;
+      double best = fabs(sm.M[k][k]);
+      for (int i = k + 1; i < n; ++i)
+        if (fabs(sm.M[i][k]) > best) { best = fabs(sm.M[i][k]); p = i; }
+      sm.piv_row = p;
+      if (best <= 1e-9 * s_scale) sm.pinned[k] = 1;
+    }
+    __syncthreads();
+    if (sm.pinned[k]) continue;  // uniform across the block
+    const int p = sm.piv_row;
+    if (p != k)
+      for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) {
+        double* rk = j < n ? &sm.M[k][j] : &sm.X[k][j - n];
+        double* rp = j < n ? &sm.M[p][j] : &sm.X[p][j - n];
+        const double t = *rk; *rk = *rp; *rp = t;
+      }
+    __syncthreads();
+    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) sm.f[i] = sm.M[i][k] / sm.M[k][k];
+    __syncthreads();
+    const int rows = n - k - 1;
+    for (int t = threadIdx.x; t < rows * 2 * n; t += blockDim.x) {
+      const int i = k + 1 + t / (2 * n), j = t % (2 * n);
+      if (j < n) {
+        if (j >= k) sm.M[i][j] -= sm.f[i] * sm.M[k][j];
+      } else {
+        sm.X[i][j - n] -= sm.f[i] * sm.X[k][j - n];
+      }
+    }
+    __syncthreads();
+  }
+  // back substitution of every column of X
+  for (int k = n - 1; k >= 0; --k) {
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      double v = 0.0;
+      if (!sm.pinned[k]) {
+        v = sm.X[k][c];
+        for (int j = k + 1; j < n; ++j) v -= sm.M[k][j] * sm.X[j][c];
+        v /= sm.M[k][k];
+      }
+      sm.X[k][c] = v;
+    }
+    __syncthreads();
+  }
+  double* out = cinv + (size_t)s * kDense * kDense;
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) out[t] = sm.X[t / n][t % n];
+}
+
+__device__ void coarse_apply_cta(const LevDesc& A, const double* __restrict__ X) {
+  const int n = A.n;
+  if (n > kDense) {
+    if (threadIdx.x == 0) {
+      for (int sweep = 0; sweep < 40; ++sweep)
+        for (int pass = 0; pass < 2; ++pass)
+          for (int q = 0; q < n; ++q) {
+            const int i = pass == 0 ? q : n - 1 - q;
+            double v = A.bc[i];
+            for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v -= A.anb64[k] * (double)A.x[A.col[k]];
+            A.x[i] = (float)(v / A.ac64[i]);
+          }
+    }
+    __syncthreads();
+    return;
+  }
+  // b is read in full before any x is written (A.bc and A.x are distinct arrays)
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = 0.0;
+    for (int j = 0; j < n; ++j) v += X[(size_t)i * n + j] * (double)A.bc[j];
+    A.x[i] = (float)v;
+  }
+  __syncthreads();
+}
+
+__device__ void smooth_cta(const LevDesc& A, int sweeps) {
+  for (int sw = 0; sw < sweeps; ++sw)
+    for (int pass = 0; pass < 2; ++pass)
+      for (int q = 0; q < A.ncolor; ++q) {
+        const int c = pass == 0 ? q : A.ncolor - 1 - q;
+        const int s0 = A.colorStart[c], s1 = A.colorStart[c + 1];
+        for (int t = s0 + threadIdx.x; t < s1; t += blockDim.x) {
+          const int i = A.colorRows[t];
+          float v = A.bc[i];
+          for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
+          A.x[i] = v / A.ac[i];
+        }
+        __syncthreads();
+      }
+}
+
+// The small-level part of the V-cycle, one CTA per slot: levels g .. coarsest, where g is the
+// first level of the slot small enough for one CTA (levels above g run as grid-wide launches).
+// Descend with pre-smoothing, residual and restriction; apply the coarsest operator; ascend
+// with prolongation and post-smoothing. A slot whose coarsest level is 0 gets its direct solve
+// on level 0 here.
+__global__ void __launch_bounds__(1024) k_coarse_vcycle(const LevDesc* __restrict__ levTab, int ns,
+                                                        const int* __restrict__ coarsest,
+                                                        const int* __restrict__ gstart, const double* __restrict__ cinv,
+                                                        int pre, int post, const SolveCtl* __restrict__ ctl) {
+  const int s = blockIdx.x;
+  if (!ctl[s].active) return;
+  const int L = coarsest[s], g = gstart[s];
+  for (int l = g; l < L; ++l) {
+    const LevDesc& A = LEV(l, s);
+    const LevDesc& C = LEV(l + 1, s);
+    smooth_cta(A, pre);
+    for (int i = threadIdx.x; i < A.n; i += blockDim.x) {
+      float v = A.bc[i] - A.ac[i] * A.x[i];
+      for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
+      A.r[i] = v;
+    }
+    __syncthreads();
+    for (int P = threadIdx.x; P < C.n; P += blockDim.x) {
+      float v = 0.0f;
+      for (int q = A.childStart[P]; q < A.childStart[P + 1]; ++q) v = v + A.r[A.child[q]];
+      C.bc[P] = v;
+      C.x[P] = 0.0f;
+    }
+    __syncthreads();
+  }
+  coarse_apply_cta(LEV(L, s), cinv + (size_t)s * kDense * kDense);
+  for (int l = L - 1; l >= g; --l) {
+    const LevDesc& A = LEV(l, s);
+    const LevDesc& C = LEV(l + 1, s);
+    for (int i = threadIdx.x; i < A.n; i += blockDim.x) A.x[i] = A.x[i] + C.x[A.parents[i]];
+    __syncthreads();
+    smooth_cta(A, post);
+  }
+}
+
+// ---------------------------------------------------------------- host side
+static int upload_work(DArr<int2>& d, const std::vector<int2>& h, cudaStream_t st) {
+  UFVM_CHECK(dalloc(d, std::max<size_t>(h.size(), 1)));
+  if (!h.empty()) UFVM_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+  return UFVM_OK;
+}
+
+template <typename T>
+static int upload_vec(DArr<T>& d, const std::vector<T>& h, cudaStream_t st) {
+  UFVM_CHECK(dalloc(d, std::max<size_t>(h.size(), 1)));
+  if (!h.empty()) UFVM_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return UFVM_OK;
+}
+
+// blocks of n items for every slot passing `use`, with per-slot entry ranges
+template <typename F>
+static void build_list(int ns, F count, std::vector<int2>& out, std::vector<int>* st, std::vector<int>* en) {
+  out.clear();
+  if (st) { st->assign(ns, 0); en->assign(ns, 0); }
+  for (int s = 0; s < ns; ++s) {
+    const int n = count(s);
+    if (st) (*st)[s] = (int)out.size();
+    for (int b = 0; b < nblocks(n); ++b) out.push_back(make_int2(s, b));
+    if (st) (*en)[s] = (int)out.size();
+  }
+}
+
+int Service::rebuild_tables() {
+  const int ns = (int)cases.size();
+  if (ns == 0) { tables_dirty = false; return UFVM_OK; }
+  UFVM_CHECK(dalloc(scal, (size_t)ns * SCAL_SLOT_N));
+  UFVM_CHECK(dalloc(flags, (size_t)ns * FLAG_N));
+  UFVM_CHECK(dalloc(uctl, ns));
+  UFVM_CHECK(dalloc(pctl, ns));
+  UFVM_CHECK(dalloc(anyflag, 4));
+  std::vector<SlotDesc> h(ns);
+  for (int s = 0; s < ns; ++s) {
+    h[s] = cases[s]->desc();
+    h[s].rowsU = cases[s]->rowsU;
+    h[s].scal = scal.p + (size_t)s * SCAL_SLOT_N;
+    h[s].flags = flags.p + (size_t)s * FLAG_N;
+  }
+  UFVM_CHECK(upload_vec(slotTab, h, stream));
+  std::vector<int2> v;
+  std::vector<int> a, b;
+  build_list(ns, [&](int s) { return cases[s]->M.Nc; }, v, &a, &b);
+  nwc = (int)v.size();
+  UFVM_CHECK(upload_work(wc, v, stream));
+  UFVM_CHECK(upload_vec(cstart, a, stream));
+  UFVM_CHECK(upload_vec(cend, b, stream));
+  build_list(ns, [&](int s) { return cases[s]->M.F; }, v, nullptr, nullptr);
+  nwf = (int)v.size();
+  UFVM_CHECK(upload_work(wf, v, stream));
+  build_list(ns, [&](int s) { return cases[s]->M.Fb; }, v, nullptr, nullptr);
+  nwb = (int)v.size();
+  UFVM_CHECK(upload_work(wb, v, stream));
+  build_list(ns, [&](int s) { return cases[s]->rowsU; }, v, &a, &b);
+  nwu = (int)v.size();
+  UFVM_CHECK(upload_work(wu, v, stream));
+  UFVM_CHECK(upload_vec(ustart, a, stream));
+  UFVM_CHECK(upload_vec(uend, b, stream));
+  UFVM_CHECK(dalloc(part, 2 * (size_t)std::max(nwc, nwu) + 16));
+  UFVM_CHECK(dalloc(fcg, 4 * (size_t)nwc + 4 * (size_t)ns + 16));
+  // AMG tables (cases without a hierarchy yet count as one level)
+  Lmax = 1;
+  for (auto* c : cases) Lmax = std::max(Lmax, c->hierarchy_valid ? c->n_levels : 1);
+  std::vector<LevDesc> lt((size_t)Lmax * ns);
+  for (int l = 0; l < Lmax; ++l)
+    for (int s = 0; s < ns; ++s) {
+      LevDesc d{};
+      Case& c = *cases[s];
+      const int nl = c.hierarchy_valid ? c.n_levels : 1;
+      if (l < nl) {
+        Level& L = c.lev[l];
+        d.n = L.n; d.nnz = L.nnz; d.ncolor = L.color_valid ? L.ncolor : 0; d.coarsest = (l == nl - 1);
+        d.rowptr = L.rowptr.p; d.col = L.col.p; d.ac64 = L.ac.p; d.anb64 = L.anb.p;
+        d.ac = L.ac32.p; d.anb = L.anb32.p; d.bc = L.bc32.p; d.x = L.dphi32.p; d.r = L.r32.p;
+        d.parents = l + 1 < nl ? L.parents.p : nullptr;
+        d.childStart = l + 1 < nl ? L.childStart.p : nullptr;
+        d.child = l + 1 < nl ? L.child.p : nullptr;
+        d.colorRows = L.colorRows.p; d.colorStart = L.colorStart.p;
+        if (l == 0) { d.fr = L.fr.p; d.fp = L.fp.p; d.fq = L.fq.p; }
+      }
+      lt[(size_t)l * ns + s] = d;
+    }
+  UFVM_CHECK(upload_vec(levTab, lt, stream));
+  wrows.resize(Lmax); nwrows.assign(Lmax, 0); wsm.resize(Lmax); nwsm.assign(Lmax, 0);
+  wnc.resize(Lmax); nwnc.assign(Lmax, 0); wrc.resize(Lmax); nwrc.assign(Lmax, 0);
+  maxcol.assign(Lmax, 0); smoff.assign(Lmax, {}); smcnt.assign(Lmax, {});
+  auto nlev = [&](int q) { return cases[q]->hierarchy_valid ? cases[q]->n_levels : 1; };
+  std::vector<int> hco(ns), hg(ns);
+  maxg = 0;
+  for (int q = 0; q < ns; ++q) {
+    const int L = nlev(q) - 1;
+    int g = 0;
+    if (L > 0) {
+      g = 1;
+      while (g < L && cases[q]->lev[g].n > kCtaRows) ++g;
+    }
+    hco[q] = L;
+    hg[q] = g;
+    maxg = std::max(maxg, g);
+  }
+  UFVM_CHECK(upload_vec(dcoarsest, hco, stream));
+  UFVM_CHECK(upload_vec(dgstart, hg, stream));
+  UFVM_CHECK(dalloc(cinv, (size_t)ns * kDense * kDense));
+  for (int l = 0; l < Lmax; ++l) {
+    build_list(ns, [&](int q) { return l < nlev(q) ? cases[q]->lev[l].n : 0; }, v, nullptr, nullptr);
+    nwrows[l] = (int)v.size();
+    UFVM_CHECK(upload_work(wrows[l], v, stream));
+    build_list(ns, [&](int q) { return l < hg[q] ? cases[q]->lev[l].n : 0; }, v, nullptr, nullptr);
+    nwnc[l] = (int)v.size();
+    UFVM_CHECK(upload_work(wnc[l], v, stream));
+    build_list(ns, [&](int q) { return l < hg[q] ? cases[q]->lev[l + 1].n : 0; }, v, nullptr, nullptr);
+    nwrc[l] = (int)v.size();
+    UFVM_CHECK(upload_work(wrc[l], v, stream));
+    // smoothing lists: rows of each colour for slots with l < g
+    int mc = 0;
+    for (int q = 0; q < ns; ++q)
+      if (l < hg[q] && cases[q]->lev[l].color_valid) mc = std::max(mc, cases[q]->lev[l].ncolor);
+    maxcol[l] = mc;
+    std::vector<int2> sm;
+    smoff[l].assign(mc, 0); smcnt[l].assign(mc, 0);
+    for (int c = 0; c < mc; ++c) {
+      smoff[l][c] = (int)sm.size();
+      for (int q = 0; q < ns; ++q) {
+        Level& L = cases[q]->lev[l];
+        if (!(l < hg[q]) || !L.color_valid || c >= L.ncolor) continue;
+        const int cnt = L.h_colorStart[c + 1] - L.h_colorStart[c];
+        for (int bb = 0; bb < nblocks(cnt); ++bb) sm.push_back(make_int2(q, bb));
+      }
+      smcnt[l][c] = (int)sm.size() - smoff[l][c];
+    }
+    nwsm[l] = (int)sm.size();
+    UFVM_CHECK(upload_work(wsm[l], sm, stream));
+  }
+  // level-0 colour rows of every slot (FP64 U smoother)
+  ucolors = 0;
+  for (auto* c : cases) ucolors = std::max(ucolors, c->lev[0].color_valid ? c->lev[0].ncolor : 0);
+  std::vector<int2> uc;
+  ucol_off.assign(ucolors, 0); ucol_cnt.assign(ucolors, 0);
+  for (int c = 0; c < ucolors; ++c) {
+    ucol_off[c] = (int)uc.size();
+    for (int s = 0; s < ns; ++s) {
+      Level& L = cases[s]->lev[0];
+      if (!L.color_valid || c >= L.ncolor) continue;
+      const int cnt = L.h_colorStart[c + 1] - L.h_colorStart[c];
+      for (int bb = 0; bb < nblocks(cnt); ++bb) uc.push_back(make_int2(s, bb));
+    }
+    ucol_cnt[c] = (int)uc.size() - ucol_off[c];
+  }
+  UFVM_CHECK(upload_work(wu_col, uc, stream));
+  tables_dirty = false;
+  return UFVM_OK;
+}
+
+BatchLaunch Service::batch() {
+  return BatchLaunch{slotTab.p, wc.p, nwc, wf.p, nwf, wb.p, nwb, wu.p, nwu, cstart.p, cend.p, ustart.p, uend.p,
+                     (int)cases.size(), part.p, stream};
+}
+
+// The reference's agglomeration of the assembled p matrix, FP32 arrays and colourings.
+int Service::ensure_hierarchy(Case& c) {
+  c.amg->smoother = UFVM_SMOOTHER_MCGS; c.amg->quirks = c.S.quirks;
+  UFVM_CHECK(c.amg->build(c.lev, c.S.p_max_coarse_levels, c.S.quirks, &c.n_levels));
+  for (int l = 0; l < c.n_levels; ++l) {
+    Level& L = c.lev[l];
+    UFVM_CHECK(dalloc(L.ac32, L.n));
+    UFVM_CHECK(dalloc(L.anb32, std::max(L.nnz, 1)));
+    UFVM_CHECK(dalloc(L.bc32, L.n));
+    UFVM_CHECK(dalloc(L.dphi32, L.n));
+    UFVM_CHECK(dalloc(L.r32, L.n));
+    if (l + 1 < c.n_levels) UFVM_CHECK(build_coloring(c.lin, L));
+    if (l == 0) {
+      UFVM_CHECK(dalloc(L.fr, L.n));
+      UFVM_CHECK(dalloc(L.fp, L.n));
+      UFVM_CHECK(dalloc(L.fq, L.n));
+    }
+  }
+  c.hierarchy_valid = true;
+  tables_dirty = true;
+  return UFVM_OK;
+}
+
+int Service::solve_u() {
+  const int ns = (int)cases.size();
+  const ufvm_settings& s = S;
+  int any = 0;
+  // the first residual is taken for every slot
+  k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(uctl.p, ns);
+  k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, wc.p, uctl.p, part.p);
+  k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
+  k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 1, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
+                                SCAL_U_R1, anyflag.p);
+  UFVM_LAUNCH_CHECK();
+  for (int it = 0; it < s.u_n_iter; ++it) {
+    ++n_usweeps;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int q = 0; q < ucolors; ++q) {
+        const int c = pass == 0 ? q : ucolors - 1 - q;
+        if (ucol_cnt[c] == 0) continue;
+        k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
+      }
+    k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, wc.p, uctl.p, part.p);
+    k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
+    k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 0, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
+                                  SCAL_U_R1, anyflag.p);
+    UFVM_LAUNCH_CHECK();
+    if (it & 1) {
+      UFVM_CUDA(cudaMemcpyAsync(&any, anyflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      UFVM_CUDA(cudaStreamSynchronize(stream));
+      if (!any) break;
+    }
+  }
+  return UFVM_OK;
+}
+
+int Service::solve_p() {
+  const int ns = (int)cases.size();
+  const ufvm_settings& s = S;
+  k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(pctl.p, ns);
+  // FP32 copy of level 0 and FP64 Galerkin products, then their FP32 copies
+  k_lev_to32<<<nwrows[0], kBlock, 0, stream>>>(levTab.p, ns, 0, wrows[0].p, pctl.p);
+  for (int l = 0; l + 1 < Lmax; ++l) {
+    k_galerkin_b<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l, wrows[l + 1].p, pctl.p);
+    k_lev_to32<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l + 1, wrows[l + 1].p, pctl.p);
+  }
+  UFVM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(DenseFactorSmem)));
+  k_coarse_factor<<<ns, 1024, sizeof(DenseFactorSmem), stream>>>(levTab.p, ns, dcoarsest.p, cinv.p);
+  UFVM_LAUNCH_CHECK();
+  k_res64_rhs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, part.p);
+  k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
+  k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, pctl.p, 1, s.p_max_cycles, s.p_termination, 0,
+                                SCAL_P_R0, SCAL_P_R1, anyflag.p);
+  UFVM_LAUNCH_CHECK();
+  auto smooth = [&](int l, int sweeps) {
+    for (int k = 0; k < sweeps; ++k)
+      for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < maxcol[l]; ++q) {
+          const int c = pass == 0 ? q : maxcol[l] - 1 - q;
+          if (smcnt[l][c] == 0) continue;
+          k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+        }
+  };
+  // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
+  const size_t o_zs = ((size_t)nwc + 1) & ~(size_t)1, o_pp = (o_zs + ns + 1) & ~(size_t)1,
+               o_ps = o_pp + 2 * (size_t)nwc;
+  double* zq_part = fcg.p;
+  double* zq_sum = fcg.p + o_zs;
+  double2* pqr_part = reinterpret_cast<double2*>(fcg.p + o_pp);
+  double2* pqr_sum = reinterpret_cast<double2*>(fcg.p + o_ps);
+  int any = 1;
+  for (int cyc = 0; cyc < s.p_max_cycles; ++cyc) {
+    ++n_pcycles;
+    // large levels as grid-wide launches, the small ones per slot in one CTA
+    for (int l = 0; l < maxg; ++l) {
+      smooth(l, s.p_pre_sweep);
+      k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+      k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
+    }
+    k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
+                                             s.p_post_sweep, pctl.p);
+    for (int l = maxg - 1; l >= 0; --l) {
+      k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+      smooth(l, s.p_post_sweep);
+    }
+    if (s.p_krylov) {
+      k_fcg_zq<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_part);
+      k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, zq_part, zq_sum);
+      k_fcg_p<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_sum, pqr_sum);
+      k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, pqr_part);
+      k_slot_sum2<<<ns, 256, 0, stream>>>(cstart.p, cend.p, pqr_part, pqr_sum);
+      k_fcg_update<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, pqr_sum, part.p);
+    } else {
+      k_update64<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p);
+      k_res64_rhs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, part.p);
+    }
+    k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
+    k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, pctl.p, 0, s.p_max_cycles, s.p_termination, 0,
+                                  SCAL_P_R0, SCAL_P_R1, anyflag.p);
+    UFVM_LAUNCH_CHECK();
+    if (cyc & 1) {
+      UFVM_CUDA(cudaMemcpyAsync(&any, anyflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      UFVM_CUDA(cudaStreamSynchronize(stream));
+      if (!any) break;
+    }
+  }
+  return UFVM_OK;
+}
+
+// One steady SIMPLE iteration of every resident case (cfdRunCase.m:92-142 order).
+int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
+  const int ns = (int)cases.size();
+  res.assign((size_t)ns * 16, 0.0);
+  conv.assign(ns, 0);
+  if (ns == 0) return UFVM_OK;
+  for (auto* c : cases) {
+    UFVM_CHECK(c->fresh_level0());
+    if (!c->lev[0].color_valid) { UFVM_CHECK(build_coloring(c->lin, c->lev[0])); tables_dirty = true; }
+  }
+  if (tables_dirty) UFVM_CHECK(rebuild_tables());
+  UFVM_CUDA(cudaMemsetAsync(flags.p, 0, (size_t)ns * FLAG_N * sizeof(int), stream));
+  ++n_iter_calls;
+  // phase timing: an event per phase boundary, read once after the final sync
+  std::vector<std::pair<int, int>> marks;  // (phase, event index)
+  int evn = 0;
+  std::vector<cudaEvent_t>& evs = evpool;
+  auto mark = [&](int phase) -> int {
+    if ((int)evs.size() <= evn) { cudaEvent_t e; if (cudaEventCreate(&e) != cudaSuccess) return UFVM_E_CUDA; evs.push_back(e); }
+    UFVM_CUDA(cudaEventRecord(evs[evn], stream));
+    marks.push_back({phase, evn++});
+    return UFVM_OK;
+  };
+  BatchLaunch b = batch();
+  UFVM_CHECK(mark(PH_UPDATE));
+  UFVM_CHECK(stage_update_fields(b));
+  for (int comp = 0; comp < 3; ++comp) {
+    UFVM_CHECK(mark(PH_ASM_U));
+    UFVM_CHECK(stage_assemble_u(b, comp));
+    k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_RMS, SCAL_U_RMS + comp);
+    k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_MAX, SCAL_U_MAX + comp);
+    UFVM_CHECK(mark(PH_SOLVE_U));
+    UFVM_CHECK(solve_u());
+    UFVM_CHECK(mark(PH_CORR_U));
+    UFVM_CHECK(stage_correct_u(b, comp));
+  }
+  int maxp = 0;
+  for (auto* c : cases) maxp = std::max(maxp, c->P.n);
+  for (int k = 0; k < S.n_correctors; ++k) {
+    UFVM_CHECK(mark(PH_ASM_P));
+    UFVM_CHECK(stage_assemble_p(b));
+    k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_RMS, SCAL_P_RMS);
+    k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_MAX, SCAL_P_MAX);
+    UFVM_CHECK(mark(PH_HIER));
+    bool built = false;
+    for (auto* c : cases) {
+      const bool rebuild = !c->hierarchy_valid ||
+                           (S.hierarchy_reuse > 0 && c->p_solves > 0 && (c->p_solves % S.hierarchy_reuse) == 0);
+      if (rebuild) { UFVM_CHECK(ensure_hierarchy(*c)); built = true; }
+      c->p_solves++;
+    }
+    if (built) {
+      UFVM_CHECK(rebuild_tables());
+      b = batch();
+    }
+    UFVM_CHECK(mark(PH_SOLVE_P));
+    UFVM_CHECK(solve_p());
+    UFVM_CHECK(mark(PH_CORR_P));
+    UFVM_CHECK(stage_correct_p(b, maxp, nullptr));
+  }
+  UFVM_CHECK(mark(PH_N));
+  // rows written by an outlet with fixed p change the scale domain (Q12)
+  for (auto* c : cases) {
+    const int before = c->rowsU;
+    for (int ip = 0; ip < c->P.n; ++ip)
+      if (c->P.type[ip] == UFVM_PATCH_OUTLET && c->P.bcP[ip] == UFVM_BC_FIXED_VALUE && c->P.count[ip] > 0) {
+        const int row0 = (c->S.quirks & UFVM_Q12_OUTLET_U_FACE_ROWS) ? c->P.start[ip] : c->M.Nc + c->P.start[ip] - c->M.Fi;
+        c->rowsU = std::max(c->rowsU, row0 + c->P.count[ip]);
+      }
+    if (c->rowsU != before) tables_dirty = true;
+  }
+  std::vector<double> h((size_t)ns * SCAL_SLOT_N);
+  std::vector<int> fl((size_t)ns * FLAG_N);
+  UFVM_CUDA(cudaMemcpyAsync(h.data(), scal.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  UFVM_CUDA(cudaMemcpyAsync(fl.data(), flags.p, fl.size() * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  UFVM_CUDA(cudaStreamSynchronize(stream));
+  for (size_t q = 0; q + 1 < marks.size(); ++q) {
+    float ms = 0;
+    UFVM_CUDA(cudaEventElapsedTime(&ms, evs[marks[q].second], evs[marks[q + 1].second]));
+    ph_ms[marks[q].first] += ms;
+  }
+  for (int q = 0; q < ns; ++q) {
+    const double* x = &h[(size_t)q * SCAL_SLOT_N];
+    double* r = &res[(size_t)q * 16];
+    for (int c = 0; c < 3; ++c) { r[c] = x[SCAL_U_RMS + c]; r[4 + c] = x[SCAL_U_MAX + c]; }
+    r[3] = x[SCAL_P_RMS]; r[7] = x[SCAL_P_MAX];
+    r[8] = x[SCAL_U_R0]; r[12] = x[SCAL_U_R1]; r[11] = x[SCAL_P_R0]; r[15] = x[SCAL_P_R1];
+    r[9] = x[SCAL_CYC];
+    const ufvm_settings& cs = cases[q]->S;
+    conv[q] = (r[0] <= cs.tol_u && r[1] <= cs.tol_u && r[2] <= cs.tol_u && r[3] <= cs.tol_p) ? 1 : 0;
+    if (fl[(size_t)q * FLAG_N + FLAG_ZERO_DIAG]) conv[q] = -UFVM_E_ZERO_DIAG;
+    if (fl[(size_t)q * FLAG_N + FLAG_BAD_BC]) conv[q] = -UFVM_E_BC_UNSUPPORTED;
+    for (int i = 0; i < 4; ++i)
+      if (std::isnan(r[i])) conv[q] = -UFVM_E_NAN;
+  }
+  return UFVM_OK;
+}
+
+Service::~Service() {
+  for (auto* c : cases) delete c;
+  cases.clear();
+  for (auto* a : {&scal, &part, &fcg}) dfree(*a);
+  dfree(flags); dfree(cstart); dfree(cend); dfree(ustart); dfree(uend); dfree(anyflag);
+  dfree(slotTab); dfree(levTab); dfree(uctl); dfree(pctl);
+  for (auto* a : {&wc, &wf, &wb, &wu, &wu_col}) dfree(*a);
+  for (auto& a : wrows) dfree(a);
+  for (auto& a : wsm) dfree(a);
+  for (auto& a : wnc) dfree(a);
+  for (auto& a : wrc) dfree(a);
+  dfree(dcoarsest); dfree(dgstart); dfree(cinv);
+  lin.release();
+  for (auto e : evpool) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace ufvm

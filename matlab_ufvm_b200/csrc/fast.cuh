@@ -1,0 +1,83 @@
+// fast.cuh -- the batched service: many resident cases advance together, one launch per
+// stage; U is smoothed with FP64 multicolour Gauss-Seidel and p is solved with FP32 AMG
+// V-cycles inside FP64 iterative refinement (FP64 residual r = b - A x, FP64 update).
+#pragma once
+#include "amg.cuh"
+#include "simple.cuh"
+
+namespace ufvm {
+
+// One (slot, AMG level) of the batched hierarchy.
+struct LevDesc {
+  int n, nnz, ncolor, coarsest;
+  const int *rowptr, *col;
+  double *ac64, *anb64;          // FP64 values (Galerkin source, coarsest direct solve)
+  float *ac, *anb, *bc, *x, *r;  // FP32 smoother arrays
+  const int* parents;            // this level -> next coarser level
+  const int *childStart, *child; // children in this level of each next-level row
+  const int *colorRows, *colorStart;
+  double *fr, *fp, *fq;          // level 0 only: FP64 flexible-CG vectors
+};
+
+// Per-slot control state of the batched linear solves (device resident).
+struct SolveCtl {
+  double r0, r1;
+  int iters, active;
+};
+
+enum { SCAL_U_RMS = 4, SCAL_P_RMS = 7, SCAL_U_MAX = 8, SCAL_P_MAX = 11, SCAL_U_R0 = 12, SCAL_P_R0 = 15,
+       SCAL_U_R1 = 16, SCAL_P_R1 = 19, SCAL_CYC = 20, SCAL_SLOT_N = 24 };
+
+struct Service {
+  ufvm_settings S{};
+  cudaStream_t stream = nullptr;
+  int nsm = 148;
+  std::vector<Case*> cases;        // resident slots (owned)
+  std::vector<long long> tickets;  // caller ids per slot
+  bool tables_dirty = true;
+  int Lmax = 1;
+  // device tables and work lists
+  DArr<SlotDesc> slotTab;
+  DArr<LevDesc> levTab;            // [Lmax][nslots]
+  DArr<double> scal;               // [nslots][SCAL_SLOT_N]
+  DArr<int> flags;                 // [nslots][FLAG_N]
+  DArr<SolveCtl> uctl, pctl;
+  DArr<double> part;
+  DArr<double> fcg;                // flexible-CG block partials and per-slot sums
+  DArr<int2> wc, wf, wb, wu;
+  int nwc = 0, nwf = 0, nwb = 0, nwu = 0;
+  DArr<int> cstart, cend, ustart, uend;
+  // AMG work lists. A slot's levels 0 .. g-1 run as grid-wide launches (smoothing, residual,
+  // restriction, prolongation), its levels g .. coarsest inside one CTA (k_coarse_vcycle).
+  // wrows[l]: rows of level l (all slots that have level l); wsm[l]: smoothing rows of level l
+  // by colour, wnc[l]: rows of level l, wrc[l]: rows of level l + 1, each for slots with l < g.
+  std::vector<DArr<int2>> wrows, wsm, wnc, wrc;
+  std::vector<int> nwrows, nwsm, nwnc, nwrc;
+  int maxg = 0;                      // max over slots of g
+  DArr<int> dcoarsest;               // per slot: index of its coarsest level
+  DArr<int> dgstart;                 // per slot: g
+  DArr<double> cinv;                 // per slot: coarsest-level solution operator (64 x 64)
+  std::vector<int> maxcol;           // per level: max colours over smoothing slots
+  std::vector<std::vector<int>> smoff;  // [level][colour] offset into wsm[level]
+  std::vector<std::vector<int>> smcnt;
+  DArr<int2> wu_col;                 // level-0 colour rows, all slots, FP64 U smoother
+  std::vector<int> ucol_off, ucol_cnt;
+  int ucolors = 0;
+  LinCtx lin;
+  DArr<int> anyflag;
+  // per-phase device time (ms) and counters, accumulated over iterate() calls
+  enum { PH_UPDATE, PH_ASM_U, PH_SOLVE_U, PH_CORR_U, PH_ASM_P, PH_HIER, PH_SOLVE_P, PH_CORR_P, PH_N };
+  double ph_ms[PH_N] = {0};
+  long long n_usweeps = 0, n_pcycles = 0, n_iter_calls = 0;
+  std::vector<cudaEvent_t> evpool;
+
+  int rebuild_tables();
+  BatchLaunch batch();
+  int ensure_hierarchy(Case& c);
+  int solve_u();
+  int solve_p();
+  int iterate(std::vector<double>& res_out, std::vector<int>& converged);
+  ~Service();
+};
+
+}  // namespace ufvm

@@ -5,7 +5,7 @@
 //                 arithmetic to the sequential sweep because a row's lower neighbours sit in
 //                 earlier levels and its upper neighbours in later ones)
 //   DILU ('ILU')  solve/cfdFactorizeILU.m:5-47, solve/cfdSolveILU.m:18-93 (level scheduled)
-//   MCGS          multicolour symmetric GS (deterministic Jones-Plassmann colouring)
+//   MCGS          multicolour symmetric GS (greedy first-fit colouring in natural order)
 //   smoother loop solve/cfdSolveAlgebraicSystem.m:11-66
 //   restriction   solve/AMG/cfdUpdateRHS.m:10-17, prolongation cfdCorrectFinerLevelSolution.m:11-14
 //
@@ -404,53 +404,38 @@ int ilu_sweep(LinCtx& c, Level& L) {
 }
 
 // ---------------------------------------------------------------- colouring + MCGS
-__device__ __forceinline__ unsigned int lowbias32(unsigned int x) {
-  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
-  return x;
-}
-
-__global__ void k_color_select(int n, const int* __restrict__ rp, const int* __restrict__ col,
-                               const int* __restrict__ color, int* sel, int* remaining) {
+// Greedy first-fit colouring in natural order, computed in dependency rounds: a row takes
+// the smallest colour unused by its lower-index neighbours once all of them are coloured.
+// A row's colour depends only on its lower neighbours' final colours, so the result is the
+// sequential greedy colouring whatever the round in which a row is reached.
+__global__ void k_greedy_round(int n, const int* __restrict__ rp, const int* __restrict__ col, int* color,
+                               int* remaining) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  sel[i] = 0;
-  if (color[i] >= 0) return;
-  const unsigned int hi = lowbias32((unsigned int)i);
-  bool top = true;
-  for (int k = rp[i]; k < rp[i + 1] && top; ++k) {
-    const int j = col[k];
-    if (j == i || color[j] >= 0) continue;
-    const unsigned int hj = lowbias32((unsigned int)j);
-    if (hj > hi || (hj == hi && j > i)) top = false;
-  }
-  if (top) sel[i] = 1;
-  atomicAdd(remaining, 1);
-}
-
-__global__ void k_color_assign(int n, const int* __restrict__ rp, const int* __restrict__ col,
-                               const int* __restrict__ sel, int* color, int* ncolor) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !sel[i]) return;
-  // smallest colour not used by an already coloured neighbour (bitmask over 64 colours,
-  // then linear probing beyond)
+  if (i >= n || __ldcg(color + i) >= 0) return;
   unsigned long long used = 0;
-  int cmax = -1;
+  bool big = false;
   for (int k = rp[i]; k < rp[i + 1]; ++k) {
-    const int cj = color[col[k]];
-    if (cj >= 0 && cj < 64) used |= 1ull << cj;
-    cmax = max(cmax, cj);
+    const int j = col[k];
+    if (j >= i) continue;
+    const int cj = __ldcg(color + j);
+    if (cj < 0) { atomicAdd(remaining, 1); return; }
+    if (cj < 64) used |= 1ull << cj;
+    else big = true;
   }
-  int c = -1;
-  if (~used) c = __ffsll(~used) - 1;
-  if (c < 0 || c >= 64) {
-    for (c = 64;; ++c) {
+  int c = ~used ? __ffsll(~used) - 1 : 64;
+  if (c >= 64 || big) {
+    for (c = 0;; ++c) {
       bool hit = false;
-      for (int k = rp[i]; k < rp[i + 1] && !hit; ++k) hit = color[col[k]] == c;
+      for (int k = rp[i]; k < rp[i + 1] && !hit; ++k) hit = col[k] < i && __ldcg(color + col[k]) == c;
       if (!hit) break;
     }
   }
-  color[i] = c;
-  atomicMax(ncolor, c + 1);
+  __stcg(color + i, c);
+}
+
+__global__ void k_max_color(int n, const int* __restrict__ color, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicMax(out, color[i] + 1);
 }
 
 int build_coloring(LinCtx& c, Level& L) {
@@ -458,23 +443,23 @@ int build_coloring(LinCtx& c, Level& L) {
   UFVM_CHECK(c.ensure(L.n));
   const int n = L.n;
   UFVM_CHECK(dalloc(L.color, n));
-  DArr<int> sel;
-  UFVM_CHECK(dalloc(sel, n));
   UFVM_CUDA(cudaMemsetAsync(L.color.p, 0xff, n * sizeof(int), c.stream));
-  UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 2, 0, sizeof(int), c.stream));
-  // Each round colours (at least) the highest-priority uncoloured row, so n rounds bound it.
-  for (int round = 0; round <= n; ++round) {
+  for (int round = 0;; round += 8) {
     UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), c.stream));
-    k_color_select<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, L.color.p, sel.p, c.iflag.p);
-    k_color_assign<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, sel.p, L.color.p, c.iflag.p + 2);
-    UFVM_LAUNCH_CHECK();
-    if ((round & 7) == 7 || round == n) {
-      int rem = 0;
-      UFVM_CUDA(cudaMemcpyAsync(&rem, c.iflag.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-      UFVM_CUDA(cudaStreamSynchronize(c.stream));
-      if (rem == 0) break;
+    for (int k = 0; k < 8; ++k) {
+      if (k == 7) UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), c.stream));
+      k_greedy_round<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, L.col.p, L.color.p, c.iflag.p);
     }
+    UFVM_LAUNCH_CHECK();
+    int rem = 0;
+    UFVM_CUDA(cudaMemcpyAsync(&rem, c.iflag.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    UFVM_CUDA(cudaStreamSynchronize(c.stream));
+    if (rem == 0) break;
+    if (round > n + 8) { set_error("colouring rounds did not terminate"); return UFVM_E_INVALID; }
   }
+  UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 2, 0, sizeof(int), c.stream));
+  k_max_color<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.color.p, c.iflag.p + 2);
+  UFVM_LAUNCH_CHECK();
   int nc = 0;
   UFVM_CUDA(cudaMemcpyAsync(&nc, c.iflag.p + 2, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   UFVM_CUDA(cudaStreamSynchronize(c.stream));
@@ -495,7 +480,7 @@ int build_coloring(LinCtx& c, Level& L) {
   UFVM_CUDA(cudaMemcpyAsync(L.h_colorStart.data(), L.colorStart.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost,
                             c.stream));
   UFVM_CUDA(cudaStreamSynchronize(c.stream));
-  dfree(cnt); dfree(sel);
+  dfree(cnt);
   L.color_valid = true;
   return UFVM_OK;
 }

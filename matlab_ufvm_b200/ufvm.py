@@ -62,7 +62,7 @@ class Settings(ct.Structure):
     _fields_ = [(n, ct.c_int32) for n in (
         "n_correctors", "fixed_element", "p_cycle", "p_max_cycles", "p_max_coarse_levels", "p_pre_sweep",
         "p_post_sweep", "p_smoother", "u_smoother", "u_n_iter", "quirks", "p_amg", "precision",
-        "hierarchy_reuse", "reserved0", "reserved1")] + [(n, ct.c_double) for n in (
+        "hierarchy_reuse", "p_krylov", "reserved1")] + [(n, ct.c_double) for n in (
             "nu", "urf_u", "urf_p", "tol_u", "tol_p", "p_termination", "u_rrf", "false_dt")]
 
 
@@ -358,3 +358,124 @@ def cfdAgglomerateLevel(rowptr, col, ac, anb):
     k, q = nc.value, cnnz.value
     return (par.cpu().numpy(), crp[:k + 1].cpu().numpy(), ccol[:q].cpu().numpy(), cac[:k].cpu().numpy(),
             canb[:q].cpu().numpy())
+
+
+# ---------------------------------------------------------------- batched service
+def _service_lib():
+    L = lib()
+    if not getattr(L, "_svc_ready", False):
+        L.ufvm_service_create.argtypes = [ct.POINTER(Settings), ct.c_int64, ct.POINTER(VP)]
+        L.ufvm_service_submit.argtypes = [VP, ct.POINTER(MeshDesc), ct.c_double, I32, I32, D, D, ct.c_int32,
+                                          ct.POINTER(ct.c_int64)]
+        L.ufvm_service_step.argtypes = [VP, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int64)]
+        L.ufvm_service_status.argtypes = [VP, ct.c_int64, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32),
+                                          ct.POINTER(ct.c_int32), D, D, D]
+        L.ufvm_service_get_field.argtypes = [VP, ct.c_int64, ct.c_char_p, D, ct.c_int64, ct.POINTER(ct.c_int64)]
+        L.ufvm_service_release.argtypes = [VP, ct.c_int64]
+        L.ufvm_service_destroy.argtypes = [VP]
+        L.ufvm_service_stats.argtypes = [VP, D, ct.c_int]
+        L._svc_ready = True
+    return L
+
+
+def fast_settings(spec: _case.CaseSpec, hierarchy_reuse: int = 1000000, p_krylov: int = 1) -> Settings:
+    """Service settings: the case's SIMPLE settings with multicolour GS and FP32 AMG
+    (p_krylov 1: the FP32 V-cycle preconditions a flexible CG in FP64)."""
+    s = settings_from_spec(spec, precision=1, hierarchy_reuse=hierarchy_reuse)
+    s.p_krylov = p_krylov
+    s.p_smoother = _case.SMOOTHER["MCGS"]
+    s.u_smoother = _case.SMOOTHER["MCGS"]
+    s.p_cycle = _case.CYCLE["V-Cycle"]
+    return s
+
+
+class Service:
+    """Continuous-batching steady-case service (ufvm_service_* in include/ufvm.h)."""
+
+    STATES = {0: "queued", 1: "resident", 2: "converged", 3: "stopped"}
+
+    def __init__(self, settings: Settings, max_resident_cells: int = 8_000_000):
+        L = _service_lib()
+        self.settings = settings
+        h = VP()
+        _check(L.ufvm_service_create(ct.byref(settings), int(max_resident_cells), ct.byref(h)))
+        self.h = h
+        self._specs = {}
+
+    def submit(self, spec: _case.CaseSpec, max_iter: int = 5000) -> int:
+        L = _service_lib()
+        m = spec.mesh
+        k = dict(pts=np.ascontiguousarray(m.points, dtype=np.float64),
+                 fs=np.ascontiguousarray(m.face_start, dtype=np.int32),
+                 fn=np.ascontiguousarray(m.face_nodes, dtype=np.int32),
+                 own=np.ascontiguousarray(m.owner, dtype=np.int32),
+                 nei=np.ascontiguousarray(m.neighbour, dtype=np.int32), pt=spec.patch_types(),
+                 ps=np.array([p.start for p in m.patches], dtype=np.int32),
+                 pn=np.array([p.n for p in m.patches], dtype=np.int32))
+        md = MeshDesc(k["pts"].shape[0], _dp(k["pts"]), k["own"].shape[0], _ip(k["fs"]), _ip(k["fn"]),
+                      k["nei"].shape[0], _ip(k["own"]), _ip(k["nei"]), len(m.patches), _ip(k["pt"]),
+                      _ip(k["ps"]), _ip(k["pn"]))
+        bu, bp = spec.bc_codes()
+        vu = np.ascontiguousarray(spec.val_u, dtype=np.float64)
+        vp = np.ascontiguousarray(spec.val_p, dtype=np.float64)
+        t = ct.c_int64()
+        _check(L.ufvm_service_submit(self.h, ct.byref(md), float(spec.nu), _ip(bu), _ip(bp), _dp(vu), _dp(vp),
+                                     int(max_iter), ct.byref(t)))
+        self._specs[t.value] = spec
+        return t.value
+
+    def step(self):
+        nr, nq, nf = ct.c_int32(), ct.c_int32(), ct.c_int64()
+        _check(_service_lib().ufvm_service_step(self.h, ct.byref(nr), ct.byref(nq), ct.byref(nf)))
+        return nr.value, nq.value, nf.value
+
+    def status(self, ticket: int) -> Dict:
+        st, code, it = ct.c_int32(), ct.c_int32(), ct.c_int32()
+        res = np.zeros(16)
+        lat, qu = ct.c_double(), ct.c_double()
+        _check(_service_lib().ufvm_service_status(self.h, ticket, ct.byref(st), ct.byref(code), ct.byref(it),
+                                                  _dp(res), ct.byref(lat), ct.byref(qu)))
+        return dict(state=self.STATES[st.value], status=code.value, iterations=it.value, res=res,
+                    latency_ms=lat.value, queue_ms=qu.value)
+
+    def field(self, ticket: int, name: str) -> np.ndarray:
+        L = _service_lib()
+        n = ct.c_int64()
+        _check(L.ufvm_service_get_field(self.h, ticket, name.encode(), None, 0, ct.byref(n)))
+        out = np.zeros(n.value)
+        _check(L.ufvm_service_get_field(self.h, ticket, name.encode(), _dp(out), n.value, ct.byref(n)))
+        return out
+
+    PHASES = ("update", "assemble_u", "solve_u", "correct_u", "assemble_p", "hierarchy", "solve_p", "correct_p")
+
+    def stats(self) -> Dict:
+        out = np.zeros(12)
+        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 12))
+        d = {f"{k}_ms": float(out[i]) for i, k in enumerate(self.PHASES)}
+        d.update(u_sweeps=int(out[8]), p_cycles=int(out[9]), steps=int(out[10]), clock_ms=float(out[11]))
+        return d
+
+    def release(self, ticket: int):
+        _check(_service_lib().ufvm_service_release(self.h, ticket))
+        self._specs.pop(ticket, None)
+
+    def run(self, max_steps: int = 100000):
+        """Step until nothing is resident or queued; returns the number of steps."""
+        steps = 0
+        while steps < max_steps:
+            nr, nq, _ = self.step()
+            steps += 1
+            if nr == 0 and nq == 0:
+                break
+        return steps
+
+    def close(self):
+        if getattr(self, "h", None):
+            _service_lib().ufvm_service_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -274,44 +274,21 @@ void ilu_sweep(int n, const int* rp, const int* col, const double* ac, const dou
   }
 }
 
-inline uint32_t lowbias32(uint32_t x) {
-  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
-  return x;
-}
-
-// Deterministic Jones-Plassmann colouring: priority (hash(i), i); in each round every
-// uncoloured row whose priority beats all uncoloured neighbours takes the smallest
-// colour unused by its already-coloured neighbours.
+// Greedy first-fit colouring in natural order: row i takes the smallest colour not used by
+// its lower-index neighbours (2 colours on the structured 2D / 3D cavities).
 int coloring(int n, const int* rp, const int* col, int* color) {
-  vector<uint32_t> h(n);
-  for (int i = 0; i < n; ++i) { h[i] = lowbias32((uint32_t)i); color[i] = -1; }
-  int remaining = n, ncolor = 0;
-  vector<int> sel;
-  vector<char> used;
-  while (remaining > 0) {
-    sel.clear();
-    for (int i = 0; i < n; ++i) {
-      if (color[i] >= 0) continue;
-      bool top = true;
-      for (int k = rp[i]; k < rp[i + 1] && top; ++k) {
-        const int j = col[k];
-        if (color[j] >= 0 || j == i) continue;
-        if (h[j] > h[i] || (h[j] == h[i] && j > i)) top = false;
-      }
-      if (top) sel.push_back(i);
+  int ncolor = 0;
+  std::vector<char> used;
+  for (int i = 0; i < n; ++i) {
+    used.assign(rp[i + 1] - rp[i] + 2, 0);
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = col[k];
+      if (j < i && color[j] < (int)used.size()) used[color[j]] = 1;
     }
-    for (int i : sel) {
-      used.assign(rp[i + 1] - rp[i] + 2, 0);
-      for (int k = rp[i]; k < rp[i + 1]; ++k) {
-        const int c = color[col[k]];
-        if (c >= 0 && c < (int)used.size()) used[c] = 1;
-      }
-      int c = 0;
-      while (used[c]) ++c;
-      color[i] = c;
-      ncolor = std::max(ncolor, c + 1);
-    }
-    remaining -= (int)sel.size();
+    int c = 0;
+    while (used[c]) ++c;
+    color[i] = c;
+    ncolor = std::max(ncolor, c + 1);
   }
   return ncolor;
 }

@@ -1,0 +1,52 @@
+"""The batched service (multicolour GS for U, FP32 AMG inside FP64 refinement for p):
+converged fields against the FP64 oracle, and each case's result alone vs in a mix."""
+import numpy as np
+import pytest
+
+from helpers import rel
+from matlab_ufvm_b200 import case
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_alone(ufvm, spec, max_iter=3000):
+    svc = ufvm.Service(ufvm.fast_settings(spec))
+    t = svc.submit(spec, max_iter)
+    svc.run()
+    st = svc.status(t)
+    return st, svc.field(t, "U"), svc.field(t, "p"), svc.field(t, "mdot")
+
+
+def test_service_converges_to_oracle_fields(ufvm_mod, oracle_mod):
+    spec = case.cavity_case(20, nu=0.01, quirks=case.QUIRKS_CONVERGING, tol_u=1e-9, tol_p=1e-12)
+    st, U, p, md = _run_alone(ufvm_mod, spec)
+    assert st["state"] == "converged", st
+    oc = oracle_mod.OracleCase(spec)
+    for it in range(3000):
+        rc, _ = oc.iterate()
+        if rc != 0:
+            break
+    assert rc == 1
+    nc = spec.mesh.n_cells
+    Uo = oc.get("U")
+    # both converged to 1e-9 scaled momentum residual: fields agree to ~1e-8
+    assert rel(U.reshape(3, -1)[:, :nc], Uo.reshape(3, -1)[:, :nc]) < 1e-7
+    assert rel(p[:nc] - p[0], oc.get("p")[:nc] - oc.get("p")[0]) < 1e-6
+
+
+def test_service_result_same_alone_and_in_mix(ufvm_mod):
+    specs = [case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(24, nu=0.005, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(6, nu=0.002, dim=3, quirks=case.QUIRKS_CONVERGING)]
+    alone = [_run_alone(ufvm_mod, s) for s in specs]
+    svc = ufvm_mod.Service(ufvm_mod.fast_settings(specs[0]), max_resident_cells=600)  # forces queueing
+    ts = [svc.submit(s, 3000) for s in specs]
+    nr, nq, nf = svc.step()
+    assert nq >= 1  # the third case waits for room
+    svc.run()
+    for t, (st, U, p, md) in zip(ts, alone):
+        s2 = svc.status(t)
+        assert s2["state"] == "converged" and s2["iterations"] == st["iterations"]
+        assert np.array_equal(svc.field(t, "U"), U)
+        assert np.array_equal(svc.field(t, "p"), p)
+        assert np.array_equal(svc.field(t, "mdot"), md)
