@@ -97,7 +97,8 @@ typedef struct {
                                   k > 0: rebuild the agglomeration every k solves */
   int32_t p_krylov;            /* service p solve: 0 plain iterative refinement (x += V(r));
                                   1 flexible CG (FCG(1)) with the FP32 V-cycle as preconditioner */
-  int32_t reserved1;
+  int32_t service_eager;       /* service tick: 0 replays one captured CUDA graph per tick, with the
+                                  solve loops ended on the device; 1 launches every kernel from the host */
   double nu;                   /* transportProperties nu */
   double urf_u, urf_p;         /* relaxationFactors */
   double tol_u, tol_p;         /* residualControl */
@@ -202,10 +203,31 @@ int ufvm_service_status(ufvm_service* s, int64_t ticket, int32_t* state, int32_t
 int ufvm_service_get_field(ufvm_service* s, int64_t ticket, const char* name, double* host, int64_t n,
                            int64_t* written);
 int ufvm_service_release(ufvm_service* s, int64_t ticket);
-/* Accumulated device time (ms) per phase -- update fields, U assembly, U solve, U correction,
- * p assembly, AMG hierarchy builds, p solve, p correction -- then the number of U smoother
- * sweeps, p V-cycles, steps and the service clock (ms). Writes min(n, 12) values. */
+/* Accumulated device time (ms) per phase of the eagerly launched ticks -- update fields,
+ * U assembly, U solve, U correction, p assembly, AMG hierarchy builds, p solve, p correction --
+ * then the number of U smoother sweeps, p V-cycles, steps, the service clock (ms), the ticks
+ * replayed as a captured graph, the number of graph captures and the kernel launches executed by
+ * the replayed graphs (loop bodies counted per execution). Writes min(n, 15) values. */
 int ufvm_service_stats(ufvm_service* s, double* out, int n);
+/* Tickets that finished (converged, stopped or failed) since the previous poll, oldest first:
+ * writes min(capacity, pending) of them and their count; the rest stay for the next poll. */
+int ufvm_service_poll(ufvm_service* s, int64_t* tickets, int64_t capacity, int64_t* n_out);
+/* Queued cases are admitted at most every `steps` steps (default 8) unless the resident cells
+ * fall to half the budget; a case's first step builds its AMG hierarchy and is launched
+ * kernel by kernel, so gathering admissions keeps the other steps on the captured graph. */
+int ufvm_service_set_admit_interval(ufvm_service* s, int32_t steps);
+/* The CUDA stream (cudaStream_t) on which the service issues all of its device work, so a
+ * caller can order its own work or timing events after a step. No counterpart in the
+ * reference (its solves are synchronous MATLAB calls). */
+int ufvm_service_stream(ufvm_service* s, void** stream);
+/* Measurement hook (no counterpart in the reference): times one kernel of the tick on the
+ * current resident batch, reps times, and returns the average device time (ms) of one unit and
+ * its compulsory DRAM bytes. kernel 0: one symmetric FP64 multicolour Gauss-Seidel sweep of
+ * every case's level 0 (the U smoother); 1: the same sweep in FP32 on the V-cycle's level 0;
+ * 2: the FP64 product q = A p of the flexible CG. The sweeps overwrite the correction vectors,
+ * which the next step's assembly resets, so call it between steps. */
+int ufvm_service_profile(ufvm_service* s, int32_t kernel, int32_t reps, double* ms_per_unit,
+                         double* bytes_per_unit);
 int ufvm_service_destroy(ufvm_service* s);
 
 const char* ufvm_last_error(void);

@@ -199,8 +199,11 @@ __global__ void k_slot_sum2(const int* __restrict__ ws, const int* __restrict__ 
 }
 
 // stopping rule of cfdSolveAlgebraicSystem / cfdApplyAMG, per slot
+// In a captured tick the same kernel also sets the condition of the solve's while node, so
+// the loop ends on the device once no slot is active.
 __global__ void k_ctrl(const SlotDesc* __restrict__ slots, int ns, const double* __restrict__ sums, SolveCtl* ctl,
-                       int first, int max_iter, double rrf, int divide_n, int r0_slot, int r1_slot, int* any) {
+                       int first, int max_iter, double rrf, int divide_n, int r0_slot, int r1_slot, int* any,
+                       int set_cond, cudaGraphConditionalHandle cond, unsigned long long* loops, int which) {
   __shared__ int sany;
   if (threadIdx.x == 0) sany = 0;
   __syncthreads();
@@ -222,7 +225,11 @@ __global__ void k_ctrl(const SlotDesc* __restrict__ slots, int ns, const double*
     if (c.active) atomicOr(&sany, 1);
   }
   __syncthreads();
-  if (threadIdx.x == 0) *any = sany;
+  if (threadIdx.x == 0) {
+    *any = sany;
+    if (!first) loops[which] += 1ull;
+    if (set_cond) cudaGraphSetConditional(cond, sany ? 1u : 0u);
+  }
 }
 
 __global__ void k_copy_scal(const SlotDesc* __restrict__ slots, int ns, int from, int to) {
@@ -538,6 +545,10 @@ int Service::rebuild_tables() {
   UFVM_CHECK(dalloc(uctl, ns));
   UFVM_CHECK(dalloc(pctl, ns));
   UFVM_CHECK(dalloc(anyflag, 4));
+  if (!loopcnt.p) {
+    UFVM_CHECK(dalloc(loopcnt, 2));
+    UFVM_CUDA(cudaMemsetAsync(loopcnt.p, 0, 2 * sizeof(unsigned long long), stream));
+  }
   std::vector<SlotDesc> h(ns);
   for (int s = 0; s < ns; ++s) {
     h[s] = cases[s]->desc();
@@ -656,6 +667,9 @@ int Service::rebuild_tables() {
   }
   UFVM_CHECK(upload_work(wu_col, uc, stream));
   tables_dirty = false;
+  graph_valid = false;
+  UFVM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(DenseFactorSmem)));
   return UFVM_OK;
 }
 
@@ -687,19 +701,58 @@ int Service::ensure_hierarchy(Case& c) {
   return UFVM_OK;
 }
 
-int Service::solve_u() {
+// ---------------------------------------------------------------- graph capture helpers
+// A captured tick is one CUDA graph, stream-captured on `stream`. Every convergence-controlled
+// solve loop becomes a conditional WHILE node added to the graph being captured; its body is
+// captured on a second stream into the node's body graph, and k_ctrl in the body sets the
+// node's condition on the device. The node starts from its default condition 1 at every launch.
+int Service::loop_begin(int kind, cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  UFVM_CUDA(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cg, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive || !cg) { set_error("loop_begin outside a capture"); return UFVM_E_CUDA; }
+  std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+  UFVM_CUDA(cudaGraphConditionalHandleCreate(h, cg, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = *h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  UFVM_CUDA(cudaGraphAddNode(&node, cg, dv.empty() ? nullptr : dv.data(), dv.size(), &np));
+  UFVM_CUDA(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  bodies.push_back({kind, body});
+  if (!bstream) UFVM_CUDA(cudaStreamCreateWithFlags(&bstream, cudaStreamNonBlocking));
+  UFVM_CUDA(cudaStreamBeginCaptureToGraph(bstream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  main_stream = stream;
+  stream = bstream;  // the body's kernels are launched on the body stream
+  return UFVM_OK;
+}
+
+int Service::loop_end() {
+  stream = main_stream;
+  cudaGraph_t g = nullptr;
+  UFVM_CUDA(cudaStreamEndCapture(bstream, &g));
+  return UFVM_OK;
+}
+
+int Service::solve_u(bool g) {
   const int ns = (int)cases.size();
   const ufvm_settings& s = S;
-  int any = 0;
+  cudaGraphConditionalHandle h = 0;
   // the first residual is taken for every slot
   k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(uctl.p, ns);
   k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, wc.p, uctl.p, part.p);
   k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
+  // (in a captured tick the while node starts from its default condition 1: a body whose
+  // slots are all inactive does nothing and its k_ctrl ends the loop)
   k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 1, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
-                                SCAL_U_R1, anyflag.p);
+                                SCAL_U_R1, anyflag.p, 0, h, loopcnt.p, 0);
   UFVM_LAUNCH_CHECK();
-  for (int it = 0; it < s.u_n_iter; ++it) {
-    ++n_usweeps;
+  auto body = [&]() -> int {
     for (int pass = 0; pass < 2; ++pass)
       for (int q = 0; q < ucolors; ++q) {
         const int c = pass == 0 ? q : ucolors - 1 - q;
@@ -709,8 +762,20 @@ int Service::solve_u() {
     k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, wc.p, uctl.p, part.p);
     k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
     k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 0, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
-                                  SCAL_U_R1, anyflag.p);
+                                  SCAL_U_R1, anyflag.p, g, h, loopcnt.p, 0);
     UFVM_LAUNCH_CHECK();
+    return UFVM_OK;
+  };
+  if (g) {
+    UFVM_CHECK(loop_begin(0, &h));
+    const int st = body();
+    UFVM_CHECK(loop_end());
+    return st;
+  }
+  int any = 0;
+  for (int it = 0; it < s.u_n_iter; ++it) {
+    ++n_usweeps;
+    UFVM_CHECK(body());
     if (it & 1) {
       UFVM_CUDA(cudaMemcpyAsync(&any, anyflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
       UFVM_CUDA(cudaStreamSynchronize(stream));
@@ -720,9 +785,10 @@ int Service::solve_u() {
   return UFVM_OK;
 }
 
-int Service::solve_p() {
+int Service::solve_p(bool g) {
   const int ns = (int)cases.size();
   const ufvm_settings& s = S;
+  cudaGraphConditionalHandle h = 0;
   k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(pctl.p, ns);
   // FP32 copy of level 0 and FP64 Galerkin products, then their FP32 copies
   k_lev_to32<<<nwrows[0], kBlock, 0, stream>>>(levTab.p, ns, 0, wrows[0].p, pctl.p);
@@ -730,14 +796,12 @@ int Service::solve_p() {
     k_galerkin_b<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l, wrows[l + 1].p, pctl.p);
     k_lev_to32<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l + 1, wrows[l + 1].p, pctl.p);
   }
-  UFVM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(DenseFactorSmem)));
   k_coarse_factor<<<ns, 1024, sizeof(DenseFactorSmem), stream>>>(levTab.p, ns, dcoarsest.p, cinv.p);
   UFVM_LAUNCH_CHECK();
   k_res64_rhs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, part.p);
   k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
   k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, pctl.p, 1, s.p_max_cycles, s.p_termination, 0,
-                                SCAL_P_R0, SCAL_P_R1, anyflag.p);
+                                SCAL_P_R0, SCAL_P_R1, anyflag.p, 0, h, loopcnt.p, 1);
   UFVM_LAUNCH_CHECK();
   auto smooth = [&](int l, int sweeps) {
     for (int k = 0; k < sweeps; ++k)
@@ -755,9 +819,7 @@ int Service::solve_p() {
   double* zq_sum = fcg.p + o_zs;
   double2* pqr_part = reinterpret_cast<double2*>(fcg.p + o_pp);
   double2* pqr_sum = reinterpret_cast<double2*>(fcg.p + o_ps);
-  int any = 1;
-  for (int cyc = 0; cyc < s.p_max_cycles; ++cyc) {
-    ++n_pcycles;
+  auto cycle = [&]() -> int {
     // large levels as grid-wide launches, the small ones per slot in one CTA
     for (int l = 0; l < maxg; ++l) {
       smooth(l, s.p_pre_sweep);
@@ -783,8 +845,20 @@ int Service::solve_p() {
     }
     k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
     k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, pctl.p, 0, s.p_max_cycles, s.p_termination, 0,
-                                  SCAL_P_R0, SCAL_P_R1, anyflag.p);
+                                  SCAL_P_R0, SCAL_P_R1, anyflag.p, g, h, loopcnt.p, 1);
     UFVM_LAUNCH_CHECK();
+    return UFVM_OK;
+  };
+  if (g) {
+    UFVM_CHECK(loop_begin(1, &h));
+    const int st = cycle();
+    UFVM_CHECK(loop_end());
+    return st;
+  }
+  int any = 1;
+  for (int cyc = 0; cyc < s.p_max_cycles; ++cyc) {
+    ++n_pcycles;
+    UFVM_CHECK(cycle());
     if (cyc & 1) {
       UFVM_CUDA(cudaMemcpyAsync(&any, anyflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
       UFVM_CUDA(cudaStreamSynchronize(stream));
@@ -794,29 +868,24 @@ int Service::solve_p() {
   return UFVM_OK;
 }
 
-// One steady SIMPLE iteration of every resident case (cfdRunCase.m:92-142 order).
-int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
+// The device work of one steady SIMPLE iteration of every resident case (cfdRunCase.m:92-142
+// order). g: being captured into the tick graph (no host synchronisation, no hierarchy
+// builds, no phase events).
+int Service::enqueue_tick(bool g, std::vector<std::pair<int, int>>& marks) {
   const int ns = (int)cases.size();
-  res.assign((size_t)ns * 16, 0.0);
-  conv.assign(ns, 0);
-  if (ns == 0) return UFVM_OK;
-  for (auto* c : cases) {
-    UFVM_CHECK(c->fresh_level0());
-    if (!c->lev[0].color_valid) { UFVM_CHECK(build_coloring(c->lin, c->lev[0])); tables_dirty = true; }
-  }
-  if (tables_dirty) UFVM_CHECK(rebuild_tables());
-  UFVM_CUDA(cudaMemsetAsync(flags.p, 0, (size_t)ns * FLAG_N * sizeof(int), stream));
-  ++n_iter_calls;
-  // phase timing: an event per phase boundary, read once after the final sync
-  std::vector<std::pair<int, int>> marks;  // (phase, event index)
   int evn = 0;
-  std::vector<cudaEvent_t>& evs = evpool;
   auto mark = [&](int phase) -> int {
-    if ((int)evs.size() <= evn) { cudaEvent_t e; if (cudaEventCreate(&e) != cudaSuccess) return UFVM_E_CUDA; evs.push_back(e); }
-    UFVM_CUDA(cudaEventRecord(evs[evn], stream));
+    if (g) return UFVM_OK;
+    if ((int)evpool.size() <= evn) {
+      cudaEvent_t e;
+      UFVM_CUDA(cudaEventCreate(&e));
+      evpool.push_back(e);
+    }
+    UFVM_CUDA(cudaEventRecord(evpool[evn], stream));
     marks.push_back({phase, evn++});
     return UFVM_OK;
   };
+  UFVM_CUDA(cudaMemsetAsync(flags.p, 0, (size_t)ns * FLAG_N * sizeof(int), stream));
   BatchLaunch b = batch();
   UFVM_CHECK(mark(PH_UPDATE));
   UFVM_CHECK(stage_update_fields(b));
@@ -826,7 +895,7 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_RMS, SCAL_U_RMS + comp);
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_MAX, SCAL_U_MAX + comp);
     UFVM_CHECK(mark(PH_SOLVE_U));
-    UFVM_CHECK(solve_u());
+    UFVM_CHECK(solve_u(g));
     UFVM_CHECK(mark(PH_CORR_U));
     UFVM_CHECK(stage_correct_u(b, comp));
   }
@@ -838,23 +907,157 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_RMS, SCAL_P_RMS);
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_MAX, SCAL_P_MAX);
     UFVM_CHECK(mark(PH_HIER));
-    bool built = false;
-    for (auto* c : cases) {
-      const bool rebuild = !c->hierarchy_valid ||
-                           (S.hierarchy_reuse > 0 && c->p_solves > 0 && (c->p_solves % S.hierarchy_reuse) == 0);
-      if (rebuild) { UFVM_CHECK(ensure_hierarchy(*c)); built = true; }
-      c->p_solves++;
-    }
-    if (built) {
-      UFVM_CHECK(rebuild_tables());
-      b = batch();
+    if (!g) {
+      bool built = false;
+      for (auto* c : cases) {
+        if (needs_hierarchy(*c)) { UFVM_CHECK(ensure_hierarchy(*c)); built = true; }
+        c->p_solves++;
+      }
+      if (built) {
+        UFVM_CHECK(rebuild_tables());
+        b = batch();
+      }
     }
     UFVM_CHECK(mark(PH_SOLVE_P));
-    UFVM_CHECK(solve_p());
+    UFVM_CHECK(solve_p(g));
     UFVM_CHECK(mark(PH_CORR_P));
     UFVM_CHECK(stage_correct_p(b, maxp, nullptr));
   }
   UFVM_CHECK(mark(PH_N));
+  return UFVM_OK;
+}
+
+bool Service::needs_hierarchy(const Case& c) const {
+  return !c.hierarchy_valid ||
+         (S.hierarchy_reuse > 0 && c.p_solves > 0 && (c.p_solves % S.hierarchy_reuse) == 0);
+}
+
+// Kernel nodes of a graph (for the launch count the service reports); -1 if the graph cannot
+// be inspected, with the error cleared so it is not taken for a failed launch later.
+static long long count_kernels(cudaGraph_t g) {
+  size_t n = 0;
+  cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "ufvm: cudaGraphGetNodes: %s\n", cudaGetErrorString(e));
+    cudaGetLastError();
+    return -1;
+  }
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n) e = cudaGraphGetNodes(g, nodes.data(), &n);
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "ufvm: cudaGraphGetNodes: %s\n", cudaGetErrorString(e));
+    cudaGetLastError();
+    return -1;
+  }
+  long long k = 0;
+  for (auto nd : nodes) {
+    // the type query fails on the conditional nodes themselves (their kernels are counted
+    // from the body graphs); such a node is skipped and the error cleared
+    cudaGraphNodeType t;
+    e = cudaGraphNodeGetType(nd, &t);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "ufvm: graph inspection left an error: %s\n", cudaGetErrorString(e));
+    return -1;
+  }
+  return k;
+}
+
+int Service::capture_tick() {
+  bodies.clear();
+  if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  graph_valid = false;
+  std::vector<std::pair<int, int>> marks;
+  UFVM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  int st = enqueue_tick(true, marks);
+  if (main_stream && stream != main_stream) {  // an error inside a loop body: close its capture
+    stream = main_stream;
+    cudaGraph_t gb = nullptr;
+    cudaStreamEndCapture(bstream, &gb);
+  }
+  cudaGraph_t gt = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(stream, &gt);
+  if (st != UFVM_OK) {
+    if (gt) cudaGraphDestroy(gt);
+    cudaGetLastError();
+    return st;
+  }
+  if (ee != cudaSuccess) {
+    set_error(std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ee));
+    cudaGetLastError();
+    return UFVM_E_CUDA;
+  }
+  graph = gt;
+  {
+    const cudaError_t pend = cudaGetLastError();
+    if (pend != cudaSuccess) std::fprintf(stderr, "ufvm: error pending after the capture: %s\n", cudaGetErrorString(pend));
+  }
+  static_kernels = count_kernels(graph);
+  ubody_kernels = pbody_kernels = 0;
+  for (auto& bb : bodies) (bb.first == 0 ? ubody_kernels : pbody_kernels) = count_kernels(bb.second);
+  bodies.clear();
+  UFVM_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+  {
+    const cudaError_t pend = cudaGetLastError();
+    if (pend != cudaSuccess) std::fprintf(stderr, "ufvm: error pending after instantiation: %s\n", cudaGetErrorString(pend));
+  }
+  graph_valid = true;
+  ++n_captures;
+  return UFVM_OK;
+}
+
+// One steady SIMPLE iteration of every resident case.
+int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
+  const int ns = (int)cases.size();
+  res.assign((size_t)ns * 16, 0.0);
+  conv.assign(ns, 0);
+  if (ns == 0) return UFVM_OK;
+  for (auto* c : cases) {
+    if (c->lev.empty() || !c->lev[0].rowptr.p) UFVM_CHECK(c->fresh_level0());
+    if (!c->lev[0].color_valid) { UFVM_CHECK(build_coloring(c->lin, c->lev[0])); tables_dirty = true; }
+  }
+  if (tables_dirty) UFVM_CHECK(rebuild_tables());
+  ++n_iter_calls;
+  // a tick without hierarchy builds runs as one graph launch (captured when the tables change)
+  bool g = use_graph != 0;
+  for (auto* c : cases) {
+    if (!g) break;
+    for (int k = 0; k < S.n_correctors; ++k) {
+      const long long ps = c->p_solves + k;
+      if (!c->hierarchy_valid || (S.hierarchy_reuse > 0 && ps > 0 && (ps % S.hierarchy_reuse) == 0)) g = false;
+    }
+  }
+  std::vector<std::pair<int, int>> marks;
+  if (g) {
+    {
+      const cudaError_t pend = cudaGetLastError();
+      if (pend != cudaSuccess) {
+        set_error(std::string("error pending before the tick: ") + cudaGetErrorString(pend));
+        return UFVM_E_CUDA;
+      }
+    }
+    if (!graph_valid && capture_tick() != UFVM_OK) {
+      // keep serving: this and later ticks are launched eagerly
+      std::fprintf(stderr, "ufvm: capturing the tick graph failed (%s); ticks are launched eagerly\n", get_error());
+      cudaGetLastError();
+      use_graph = 0;
+      g = false;
+    }
+  }
+  if (g) {
+    UFVM_CUDA(cudaGraphLaunch(gexec, stream));
+    for (auto* c : cases) c->p_solves += S.n_correctors;
+    ++n_graph_ticks;
+  } else {
+    UFVM_CHECK(enqueue_tick(false, marks));
+  }
   // rows written by an outlet with fixed p change the scale domain (Q12)
   for (auto* c : cases) {
     const int before = c->rowsU;
@@ -869,12 +1072,27 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
   std::vector<int> fl((size_t)ns * FLAG_N);
   UFVM_CUDA(cudaMemcpyAsync(h.data(), scal.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
   UFVM_CUDA(cudaMemcpyAsync(fl.data(), flags.p, fl.size() * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  unsigned long long lc[2] = {0, 0};
+  UFVM_CUDA(cudaMemcpyAsync(lc, loopcnt.p, sizeof(lc), cudaMemcpyDeviceToHost, stream));
   UFVM_CUDA(cudaStreamSynchronize(stream));
+  {
+    const cudaError_t pend = cudaGetLastError();
+    if (pend != cudaSuccess) {
+      set_error(std::string(g ? "graph tick: " : "eager tick: ") + cudaGetErrorString(pend));
+      return UFVM_E_CUDA;
+    }
+  }
+  if (g && static_kernels >= 0 && ubody_kernels >= 0 && pbody_kernels >= 0)
+    launches_total += static_kernels + ubody_kernels * (long long)(lc[0] - loops_seen[0]) +
+                      pbody_kernels * (long long)(lc[1] - loops_seen[1]);
+  loops_seen[0] = lc[0];
+  loops_seen[1] = lc[1];
   for (size_t q = 0; q + 1 < marks.size(); ++q) {
     float ms = 0;
-    UFVM_CUDA(cudaEventElapsedTime(&ms, evs[marks[q].second], evs[marks[q + 1].second]));
+    UFVM_CUDA(cudaEventElapsedTime(&ms, evpool[marks[q].second], evpool[marks[q + 1].second]));
     ph_ms[marks[q].first] += ms;
   }
+  int maxcyc = 0;
   for (int q = 0; q < ns; ++q) {
     const double* x = &h[(size_t)q * SCAL_SLOT_N];
     double* r = &res[(size_t)q * 16];
@@ -882,6 +1100,7 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
     r[3] = x[SCAL_P_RMS]; r[7] = x[SCAL_P_MAX];
     r[8] = x[SCAL_U_R0]; r[12] = x[SCAL_U_R1]; r[11] = x[SCAL_P_R0]; r[15] = x[SCAL_P_R1];
     r[9] = x[SCAL_CYC];
+    maxcyc = std::max(maxcyc, (int)r[9]);
     const ufvm_settings& cs = cases[q]->S;
     conv[q] = (r[0] <= cs.tol_u && r[1] <= cs.tol_u && r[2] <= cs.tol_u && r[3] <= cs.tol_p) ? 1 : 0;
     if (fl[(size_t)q * FLAG_N + FLAG_ZERO_DIAG]) conv[q] = -UFVM_E_ZERO_DIAG;
@@ -889,14 +1108,98 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
     for (int i = 0; i < 4; ++i)
       if (std::isnan(r[i])) conv[q] = -UFVM_E_NAN;
   }
+  if (g) n_pcycles += (long long)maxcyc * S.n_correctors;
   return UFVM_OK;
 }
 
+// Times one kernel of the tick on the current resident batch, `reps` times after one warm-up,
+// and returns the average device time of one unit and its compulsory bytes (every array
+// touched once per pass; neighbour gathers of x counted as cache hits). Units:
+//   0: one symmetric FP64 multicolour Gauss-Seidel sweep of every slot's level 0 (k_mc64,
+//      2 x colours launches): 2 x (40 B per row + 12 B per nonzero);
+//   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32): 2 x (24 B/row + 8 B/nz);
+//   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz.
+// The sweeps overwrite the slots' correction vectors, which the next assembly re-zeroes.
+int Service::profile(int kernel, int reps, double* ms, double* bytes) {
+  const int ns = (int)cases.size();
+  if (ns == 0 || reps <= 0) { set_error("profile: no resident case or reps <= 0"); return UFVM_E_INVALID; }
+  if (tables_dirty) UFVM_CHECK(rebuild_tables());
+  double N = 0, NNZ = 0;
+  for (auto* c : cases) { N += c->M.Nc; NNZ += c->M.nnz; }
+  auto unit = [&]() -> int {
+    if (kernel == 0) {
+      for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < ucolors; ++q) {
+          const int c = pass == 0 ? q : ucolors - 1 - q;
+          if (ucol_cnt[c] == 0) continue;
+          k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
+        }
+    } else if (kernel == 1) {
+      for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < maxcol[0]; ++q) {
+          const int c = pass == 0 ? q : maxcol[0] - 1 - q;
+          if (smcnt[0][c] == 0) continue;
+          k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
+        }
+    } else {
+      k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,
+                                          reinterpret_cast<double2*>(fcg.p + (((size_t)nwc + 1) & ~(size_t)1) +
+                                                                     (((size_t)ns + 1) & ~(size_t)1)));
+    }
+    UFVM_LAUNCH_CHECK();
+    return UFVM_OK;
+  };
+  if (kernel < 0 || kernel > 2) { set_error("profile: unknown kernel id"); return UFVM_E_INVALID; }
+  if (kernel >= 1) {
+    for (auto* c : cases)
+      if (!c->hierarchy_valid) { set_error("profile: a resident case has no AMG hierarchy yet"); return UFVM_E_INVALID; }
+    if (Lmax < 2 || nwsm.empty()) { set_error("profile: no AMG hierarchy yet"); return UFVM_E_INVALID; }
+  }
+  if (kernel == 1) {
+    N = 0; NNZ = 0;
+    for (auto* c : cases)
+      if (c->hierarchy_valid && c->n_levels > 1) { N += c->M.Nc; NNZ += c->M.nnz; }
+  }
+  k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(uctl.p, ns);
+  k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(pctl.p, ns);
+  UFVM_CHECK(unit());
+  cudaEvent_t a, b;
+  UFVM_CUDA(cudaEventCreate(&a));
+  UFVM_CUDA(cudaEventCreate(&b));
+  UFVM_CUDA(cudaEventRecord(a, stream));
+  for (int r = 0; r < reps; ++r) UFVM_CHECK(unit());
+  UFVM_CUDA(cudaEventRecord(b, stream));
+  UFVM_CUDA(cudaEventSynchronize(b));
+  float t = 0;
+  UFVM_CUDA(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t / reps;
+  if (kernel == 0) *bytes = 2.0 * (40.0 * N + 12.0 * NNZ);
+  else if (kernel == 1) *bytes = 2.0 * (24.0 * N + 8.0 * NNZ);
+  else *bytes = 36.0 * N + 12.0 * NNZ;
+  return UFVM_OK;
+}
+
+// Destroy calls cannot report to a caller; a failure is printed once and then cleared so that
+// it is not mistaken later for a failed launch of another case or service.
+static void destroy_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "ufvm: %s failed during service teardown: %s\n", what, cudaGetErrorString(e));
+    cudaGetLastError();
+  }
+}
+
 Service::~Service() {
+  if (stream) destroy_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+  if (gexec) destroy_check(cudaGraphExecDestroy(gexec), "cudaGraphExecDestroy");
+  if (graph) destroy_check(cudaGraphDestroy(graph), "cudaGraphDestroy");
+  gexec = nullptr;
+  graph = nullptr;
   for (auto* c : cases) delete c;
   cases.clear();
   for (auto* a : {&scal, &part, &fcg}) dfree(*a);
-  dfree(flags); dfree(cstart); dfree(cend); dfree(ustart); dfree(uend); dfree(anyflag);
+  dfree(flags); dfree(cstart); dfree(cend); dfree(ustart); dfree(uend); dfree(anyflag); dfree(loopcnt);
   dfree(slotTab); dfree(levTab); dfree(uctl); dfree(pctl);
   for (auto* a : {&wc, &wf, &wb, &wu, &wu_col}) dfree(*a);
   for (auto& a : wrows) dfree(a);
@@ -905,8 +1208,10 @@ Service::~Service() {
   for (auto& a : wrc) dfree(a);
   dfree(dcoarsest); dfree(dgstart); dfree(cinv);
   lin.release();
-  for (auto e : evpool) cudaEventDestroy(e);
-  if (stream) cudaStreamDestroy(stream);
+  for (auto e : evpool) destroy_check(cudaEventDestroy(e), "cudaEventDestroy");
+  if (bstream) destroy_check(cudaStreamDestroy(bstream), "cudaStreamDestroy");
+  if (stream) destroy_check(cudaStreamDestroy(stream), "cudaStreamDestroy");
+  destroy_check(cudaGetLastError(), "a CUDA call");
 }
 
 }  // namespace ufvm

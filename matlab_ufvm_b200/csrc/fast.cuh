@@ -71,12 +71,33 @@ struct Service {
   long long n_usweeps = 0, n_pcycles = 0, n_iter_calls = 0;
   std::vector<cudaEvent_t> evpool;
 
+  // one tick as a CUDA graph with device-side loop control (conditional WHILE nodes)
+  int use_graph = 1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_valid = false;
+  cudaStream_t bstream = nullptr;      // loop bodies are captured on this stream
+  cudaStream_t main_stream = nullptr;
+  long long n_graph_ticks = 0, n_captures = 0;
+  // kernel launches: kernels of the captured tick outside the loops and per loop body, and
+  // the device counters of executed U / p loop bodies
+  long long static_kernels = 0, ubody_kernels = 0, pbody_kernels = 0, launches_total = 0;
+  std::vector<std::pair<int, cudaGraph_t>> bodies;  // (0 U / 1 p, body graph) of the capture
+  DArr<unsigned long long> loopcnt;
+  unsigned long long loops_seen[2] = {0, 0};
+
   int rebuild_tables();
   BatchLaunch batch();
+  bool needs_hierarchy(const Case& c) const;
   int ensure_hierarchy(Case& c);
-  int solve_u();
-  int solve_p();
+  int loop_begin(int kind, cudaGraphConditionalHandle* h);
+  int loop_end();
+  int solve_u(bool g);
+  int solve_p(bool g);
+  int enqueue_tick(bool g, std::vector<std::pair<int, int>>& marks);
+  int capture_tick();
   int iterate(std::vector<double>& res_out, std::vector<int>& converged);
+  int profile(int kernel, int reps, double* ms, double* bytes);
   ~Service();
 };
 

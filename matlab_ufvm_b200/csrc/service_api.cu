@@ -30,6 +30,7 @@ struct Record {
   double t_submit = 0, t_admit = 0, t_done = 0;
   Case* c = nullptr;  // owned while resident or finished-unreleased
   long long cells = 0;
+  std::string err;    // why admission or a step failed
 };
 
 struct ServiceImpl {
@@ -39,6 +40,12 @@ struct ServiceImpl {
   std::map<long long, Record> rec;
   double clock_ms = 0;  // accumulated device time of all steps
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // admission runs at most every admit_interval steps unless the resident cells fall to half
+  // the budget: a newly admitted case's first iteration builds its AMG hierarchy, a step that
+  // cannot be replayed from the captured graph, so admissions are gathered into few steps
+  int admit_interval = 8;
+  long long steps_since_admit = 1 << 30;
+  std::vector<long long> finished_unpolled;  // tickets finished since the last poll
   ~ServiceImpl() {
     for (auto& kv : rec)
       if (kv.second.c && kv.second.state >= 2) { delete kv.second.c; kv.second.c = nullptr; }
@@ -48,6 +55,10 @@ struct ServiceImpl {
 };
 
 static int admit(ServiceImpl& S) {
+  if (S.queue.empty()) return UFVM_OK;
+  if (!S.svc.cases.empty() && S.steps_since_admit < S.admit_interval && 2 * S.resident_cells > S.max_cells)
+    return UFVM_OK;
+  const size_t before = S.svc.cases.size();
   while (!S.queue.empty()) {
     Pending& p = S.queue.front();
     const long long nc_est = (long long)(p.own.empty() ? 0 : 1);
@@ -70,11 +81,13 @@ static int admit(ServiceImpl& S) {
     Record& r = S.rec[p.ticket];
     r.t_admit = S.clock_ms;
     if (st != UFVM_OK) {
+      r.err = get_error();
       delete c;
       r.state = 3;
       r.status = st;
       r.t_done = S.clock_ms;
       ++S.finished;
+      S.finished_unpolled.push_back(p.ticket);
       S.queue.pop_front();
       continue;
     }
@@ -87,6 +100,7 @@ static int admit(ServiceImpl& S) {
     S.svc.tables_dirty = true;
     S.queue.pop_front();
   }
+  if (S.svc.cases.size() != before) S.steps_since_admit = 0;
   return UFVM_OK;
 }
 
@@ -109,6 +123,7 @@ int ufvm_service_create(const ufvm_settings* settings, int64_t max_resident_cell
   ufvm_service* h = new ufvm_service();
   ServiceImpl& S = h->impl;
   S.svc.S = *settings;
+  S.svc.use_graph = settings->service_eager ? 0 : 1;
   S.max_cells = max_resident_cells;
   if (cudaStreamCreateWithFlags(&S.svc.stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&S.e0) != cudaSuccess || cudaEventCreate(&S.e1) != cudaSuccess) {
@@ -189,6 +204,7 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
         r.t_done = S.clock_ms;
         S.resident_cells -= r.cells;
         ++S.finished;
+        S.finished_unpolled.push_back(V.tickets[q]);
         V.tables_dirty = true;
       } else {
         keep.push_back(V.cases[q]);
@@ -198,6 +214,7 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
     V.cases = keep;
     V.tickets = keept;
   }
+  ++S.steps_since_admit;
   UFVM_CHECK(admit(S));
   if (n_resident) *n_resident = (int32_t)V.cases.size();
   if (n_queued) *n_queued = (int32_t)S.queue.size();
@@ -225,7 +242,12 @@ int ufvm_service_get_field(ufvm_service* h, int64_t ticket, const char* name, do
                            int64_t* written) {
   if (!h) return UFVM_E_INVALID;
   auto it = h->impl.rec.find(ticket);
-  if (it == h->impl.rec.end() || !it->second.c) { set_error("ticket has no resident or finished case"); return UFVM_E_INVALID; }
+  if (it == h->impl.rec.end()) { set_error("unknown ticket"); return UFVM_E_INVALID; }
+  if (!it->second.c) {
+    set_error("ticket has no resident or finished case" +
+              (it->second.err.empty() ? std::string() : " (admission failed: " + it->second.err + ")"));
+    return UFVM_E_INVALID;
+  }
   // borrow the case through a temporary handle-free path
   Case& C = *it->second.c;
   const size_t R = C.M.Nc + C.M.Fb;
@@ -267,7 +289,38 @@ int ufvm_service_stats(ufvm_service* h, double* out, int n) {
   v.push_back((double)V.n_pcycles);
   v.push_back((double)V.n_iter_calls);
   v.push_back(h->impl.clock_ms);
+  v.push_back((double)V.n_graph_ticks);
+  v.push_back((double)V.n_captures);
+  v.push_back((double)V.launches_total);
   for (int i = 0; i < n; ++i) out[i] = i < (int)v.size() ? v[i] : 0.0;
+  return UFVM_OK;
+}
+
+int ufvm_service_profile(ufvm_service* h, int32_t kernel, int32_t reps, double* ms_per_unit,
+                         double* bytes_per_unit) {
+  if (!h || !ms_per_unit || !bytes_per_unit) return UFVM_E_INVALID;
+  return h->impl.svc.profile(kernel, reps, ms_per_unit, bytes_per_unit);
+}
+
+int ufvm_service_poll(ufvm_service* h, int64_t* tickets, int64_t capacity, int64_t* n_out) {
+  if (!h || !n_out || capacity < 0 || (capacity > 0 && !tickets)) return UFVM_E_INVALID;
+  auto& f = h->impl.finished_unpolled;
+  const int64_t n = std::min<int64_t>(capacity, (int64_t)f.size());
+  for (int64_t i = 0; i < n; ++i) tickets[i] = f[i];
+  f.erase(f.begin(), f.begin() + n);
+  *n_out = n;
+  return UFVM_OK;
+}
+
+int ufvm_service_set_admit_interval(ufvm_service* h, int32_t steps) {
+  if (!h || steps < 1) return UFVM_E_INVALID;
+  h->impl.admit_interval = steps;
+  return UFVM_OK;
+}
+
+int ufvm_service_stream(ufvm_service* h, void** stream) {
+  if (!h || !stream) return UFVM_E_INVALID;
+  *stream = (void*)h->impl.svc.stream;
   return UFVM_OK;
 }
 

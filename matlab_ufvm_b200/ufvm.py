@@ -28,7 +28,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import os
-from typing import Dict, Optional, Tuple
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -62,7 +62,7 @@ class Settings(ct.Structure):
     _fields_ = [(n, ct.c_int32) for n in (
         "n_correctors", "fixed_element", "p_cycle", "p_max_cycles", "p_max_coarse_levels", "p_pre_sweep",
         "p_post_sweep", "p_smoother", "u_smoother", "u_n_iter", "quirks", "p_amg", "precision",
-        "hierarchy_reuse", "p_krylov", "reserved1")] + [(n, ct.c_double) for n in (
+        "hierarchy_reuse", "p_krylov", "service_eager")] + [(n, ct.c_double) for n in (
             "nu", "urf_u", "urf_p", "tol_u", "tol_p", "p_termination", "u_rrf", "false_dt")]
 
 
@@ -374,6 +374,10 @@ def _service_lib():
         L.ufvm_service_release.argtypes = [VP, ct.c_int64]
         L.ufvm_service_destroy.argtypes = [VP]
         L.ufvm_service_stats.argtypes = [VP, D, ct.c_int]
+        L.ufvm_service_stream.argtypes = [VP, ct.POINTER(VP)]
+        L.ufvm_service_profile.argtypes = [VP, ct.c_int32, ct.c_int32, D, D]
+        L.ufvm_service_poll.argtypes = [VP, ct.POINTER(ct.c_int64), ct.c_int64, ct.POINTER(ct.c_int64)]
+        L.ufvm_service_set_admit_interval.argtypes = [VP, ct.c_int32]
         L._svc_ready = True
     return L
 
@@ -449,11 +453,34 @@ class Service:
     PHASES = ("update", "assemble_u", "solve_u", "correct_u", "assemble_p", "hierarchy", "solve_p", "correct_p")
 
     def stats(self) -> Dict:
-        out = np.zeros(12)
-        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 12))
+        out = np.zeros(15)
+        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 15))
         d = {f"{k}_ms": float(out[i]) for i, k in enumerate(self.PHASES)}
-        d.update(u_sweeps=int(out[8]), p_cycles=int(out[9]), steps=int(out[10]), clock_ms=float(out[11]))
+        d.update(u_sweeps=int(out[8]), p_cycles=int(out[9]), steps=int(out[10]), clock_ms=float(out[11]),
+                 graph_ticks=int(out[12]), captures=int(out[13]), graph_launches=int(out[14]))
         return d
+
+    def poll(self, capacity: int = 4096) -> List[int]:
+        """Tickets finished since the previous poll."""
+        buf = (ct.c_int64 * capacity)()
+        n = ct.c_int64()
+        _check(_service_lib().ufvm_service_poll(self.h, buf, capacity, ct.byref(n)))
+        return [int(buf[i]) for i in range(n.value)]
+
+    def set_admit_interval(self, steps: int):
+        _check(_service_lib().ufvm_service_set_admit_interval(self.h, int(steps)))
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) that all of the service's device work runs on."""
+        v = VP()
+        _check(_service_lib().ufvm_service_stream(self.h, ct.byref(v)))
+        return int(v.value or 0)
+
+    def profile(self, kernel: int, reps: int = 20) -> Tuple[float, float]:
+        """(ms per unit, compulsory bytes per unit) of one tick kernel on the resident batch."""
+        ms, by = ct.c_double(), ct.c_double()
+        _check(_service_lib().ufvm_service_profile(self.h, int(kernel), int(reps), ct.byref(ms), ct.byref(by)))
+        return ms.value, by.value
 
     def release(self, ticket: int):
         _check(_service_lib().ufvm_service_release(self.h, ticket))

@@ -50,3 +50,29 @@ def test_service_result_same_alone_and_in_mix(ufvm_mod):
         assert np.array_equal(svc.field(t, "U"), U)
         assert np.array_equal(svc.field(t, "p"), p)
         assert np.array_equal(svc.field(t, "mdot"), md)
+
+
+def test_service_graph_ticks_match_eager_ticks(ufvm_mod):
+    """A tick replayed as the captured graph (solve loops ended on the device) gives the
+    same bits as the same tick launched kernel by kernel from the host."""
+    specs = [case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(40, nu=0.002, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(6, nu=0.002, dim=3, quirks=case.QUIRKS_CONVERGING)]
+    out = []
+    for eager in (0, 1):
+        s = ufvm_mod.fast_settings(specs[0])
+        s.service_eager = eager
+        svc = ufvm_mod.Service(s)
+        ts = [svc.submit(x, 3000) for x in specs]
+        for _ in range(25):
+            svc.step()
+        fields = [(svc.field(t, "U"), svc.field(t, "p"), svc.field(t, "mdot")) for t in ts]
+        out.append((fields, svc.stats(), [svc.status(t)["res"] for t in ts]))
+        svc.close()
+    (fg, sg, rg), (fe, se, re_) = out
+    assert sg["graph_ticks"] >= 20 and se["graph_ticks"] == 0
+    for a, b in zip(fg, fe):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    for x, y in zip(rg, re_):
+        assert np.array_equal(x, y)
