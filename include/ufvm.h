@@ -162,6 +162,17 @@ int ufvm_compute_residuals_array(int32_t n, const int32_t* rowptr, const int32_t
 /* dphi = cfdSolveSOR(...) one symmetric natural-order Gauss-Seidel sweep (solve/cfdSolveSOR.m). */
 int ufvm_solve_sor(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
                    const double* anb, const double* bc, double* dphi, void* stream);
+/* ufvm_solve_sor without any device allocation. No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory when they call the smoother (a MEX gateway inside
+ * a caller-owned device-memory budget, an application whose pool allocator owns all device
+ * memory, or pipelined code that must not hit cudaMalloc's implicit synchronisation). All of
+ * its scratch lives in one fixed array of about 4 MiB compiled into the library, so systems of
+ * more than 262,144 rows are rejected with UFVM_E_INVALID. Every call shares that array and
+ * clears what it needs; calls whose device work overlaps race on it and must be serialised.
+ * The first call on a device looks the array up with cudaGetSymbolAddress: make it before any
+ * stream capture. Results are bit-identical to ufvm_solve_sor's. */
+int ufvm_solve_sor_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
+                           const double* anb, const double* bc, double* dphi, void* stream);
 /* [dc] = cfdFactorizeILU and dphi = cfdSolveILU (solve/cfdFactorizeILU.m, cfdSolveILU.m). */
 int ufvm_factorize_ilu(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
                        const double* anb, double* dc, int32_t quirks, void* stream);

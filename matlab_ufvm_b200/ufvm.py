@@ -99,6 +99,7 @@ def lib():
     L.ufvm_get_level_array.argtypes = [VP, ct.c_int, ct.c_char_p, VP, ct.c_int64, ct.POINTER(ct.c_int64)]
     for name, extra in (("ufvm_compute_residuals_array", [VP, VP, VP, VP, VP, VP, VP, VP]),
                         ("ufvm_solve_sor", [VP, VP, VP, VP, VP, VP, VP]),
+                        ("ufvm_solve_sor_noalloc", [VP, VP, VP, VP, VP, VP, VP]),
                         ("ufvm_solve_ilu", [VP, VP, VP, VP, VP, VP, VP, VP])):
         getattr(L, name).argtypes = [ct.c_int32] + extra
     L.ufvm_factorize_ilu.argtypes = [ct.c_int32, VP, VP, VP, VP, VP, ct.c_int32, VP]
