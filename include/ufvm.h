@@ -227,6 +227,10 @@ int ufvm_service_poll(ufvm_service* s, int64_t* tickets, int64_t capacity, int64
  * fall to half the budget; a case's first step builds its AMG hierarchy and is launched
  * kernel by kernel, so gathering admissions keeps the other steps on the captured graph. */
 int ufvm_service_set_admit_interval(ufvm_service* s, int32_t steps);
+/* Launch schedule of the p solve's V-cycle: AMG levels of at most cta_rows rows are smoothed
+ * by one thread block per case (all of a case's small levels in one launch), larger levels by
+ * grid-wide launches over all cases (default 2048). Takes effect at the next step. */
+int ufvm_service_set_schedule(ufvm_service* s, int32_t cta_rows);
 /* The CUDA stream (cudaStream_t) on which the service issues all of its device work, so a
  * caller can order its own work or timing events after a step. No counterpart in the
  * reference (its solves are synchronous MATLAB calls). */

@@ -49,6 +49,13 @@ struct Level {
   // FP64 flexible-CG vectors of the level-0 refinement (residual, search direction, A times
   // search direction)
   DArr<double> fr, fp, fq;
+  // level 0 of the batched service's FP32 V-cycle in colour-permuted ELL form: position p holds
+  // row perm[p] (colour-major, natural order inside a colour), inv is the inverse map, entry k
+  // of row p sits at [k * n + p] (column as a permuted index, -1 past the row's end)
+  bool l0_valid = false;
+  int ellW = 0;
+  DArr<int> perm, inv, ellCol, parentsP, childP;
+  DArr<float> ellAnb;
 };
 
 // Scratch buffers for matrix-level work (owned by a Case or by a stand-alone call).

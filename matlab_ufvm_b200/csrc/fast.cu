@@ -55,8 +55,9 @@ __global__ void k_res64_rhs(const SlotDesc* __restrict__ slots, const LevDesc* _
     for (int k = rp[i]; k < rp[i + 1]; ++k) r = r - S.anb[k] * S.dphi[S.m.col[k]];
     v = fabs(r);
     if (A.fr) A.fr[i] = r;
-    A.bc[i] = (float)r;
-    A.x[i] = 0.0f;
+    const int j = A.pmode ? A.inv[i] : i;
+    A.bc[j] = (float)r;
+    A.x[j] = 0.0f;
   }
   v = block_reduce<0>(v, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
@@ -68,7 +69,8 @@ __global__ void k_update64(const SlotDesc* __restrict__ slots, const LevDesc* __
   if (!ctl[w.x].active) return;
   const SlotDesc& S = slots[w.x];
   const int i = w.y * blockDim.x + threadIdx.x;
-  if (i < S.m.Nc) S.dphi[i] = S.dphi[i] + (double)LEV(0, w.x).x[i];
+  const LevDesc& A = LEV(0, w.x);
+  if (i < S.m.Nc) S.dphi[i] = S.dphi[i] + (double)A.x[A.pmode ? A.inv[i] : i];
 }
 
 // ---------------------------------------------------------------- flexible CG on level 0
@@ -88,7 +90,7 @@ __global__ void k_fcg_zq(const SlotDesc* __restrict__ slots, const LevDesc* __re
   const LevDesc& A = LEV(0, w.x);
   const int i = w.y * blockDim.x + threadIdx.x;
   double v = 0.0;
-  if (i < S.m.Nc && ctl[w.x].active && ctl[w.x].iters > 0) v = (double)A.x[i] * A.fq[i];
+  if (i < S.m.Nc && ctl[w.x].active && ctl[w.x].iters > 0) v = (double)A.x[A.pmode ? A.inv[i] : i] * A.fq[i];
   v = block_reduce<0>(v, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
@@ -103,7 +105,7 @@ __global__ void k_fcg_p(const SlotDesc* __restrict__ slots, const LevDesc* __res
   const LevDesc& A = LEV(0, w.x);
   const int i = w.y * blockDim.x + threadIdx.x;
   if (i >= S.m.Nc) return;
-  const double z = (double)A.x[i];
+  const double z = (double)A.x[A.pmode ? A.inv[i] : i];
   if (c.iters == 0) {
     A.fp[i] = z;
   } else {
@@ -150,8 +152,9 @@ __global__ void k_fcg_update(const SlotDesc* __restrict__ slots, const LevDesc* 
     S.dphi[i] = S.dphi[i] + alpha * A.fp[i];
     const double r = A.fr[i] - alpha * A.fq[i];
     A.fr[i] = r;
-    A.bc[i] = (float)r;
-    A.x[i] = 0.0f;
+    const int j = A.pmode ? A.inv[i] : i;
+    A.bc[j] = (float)r;
+    A.x[j] = 0.0f;
     v = fabs(r);
   }
   v = block_reduce<0>(v, sh);
@@ -283,6 +286,84 @@ __global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, 
   C.ac64[P] = AC;
 }
 
+// ---- level 0 of the V-cycle in colour-permuted ELL storage (pmode 1). Rows of one colour
+// are contiguous, so the row arrays are read with unit stride and every entry's column and
+// coefficient are coalesced across the warp; the only dependent load is the neighbour x.
+// Each row keeps the CSR (cconn) order of its entries.
+__global__ void k_l0_to32(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
+                          const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& A = LEV(0, w.x);
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  if (!A.pmode) {
+    A.ac[p] = (float)A.ac64[p];
+    for (int k = A.rowptr[p]; k < A.rowptr[p + 1]; ++k) A.anb[k] = (float)A.anb64[k];
+    return;
+  }
+  const int i = A.perm[p], k0 = A.rowptr[i], deg = A.rowptr[i + 1] - k0;
+  A.ac[p] = (float)A.ac64[i];
+  for (int k = 0; k < A.ellW; ++k) A.ellAnb[(size_t)k * A.n + p] = k < deg ? (float)A.anb64[k0 + k] : 0.0f;
+}
+
+__device__ __forceinline__ float l0_row_sum(const LevDesc& A, int p, float v) {
+  for (int k = 0; k < A.ellW; ++k) {
+    const int c = A.ellCol[(size_t)k * A.n + p];
+    if (c < 0) break;
+    v = v - A.ellAnb[(size_t)k * A.n + p] * A.x[c];
+  }
+  return v;
+}
+
+__global__ void k_mc32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work, int color,
+                          const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& A = LEV(0, w.x);
+  if (color >= A.ncolor) return;
+  const int s0 = A.colorStart[color], cnt = A.colorStart[color + 1] - s0;
+  const int t = w.y * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int p = s0 + t;
+  A.x[p] = l0_row_sum(A, p, A.bc[p]) / A.ac[p];
+}
+
+__global__ void k_res32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
+                           const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& A = LEV(0, w.x);
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  A.r[p] = l0_row_sum(A, p, A.bc[p] - A.ac[p] * A.x[p]);
+}
+
+__global__ void k_restrict32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
+                                const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& F = LEV(0, w.x);
+  const LevDesc& C = LEV(1, w.x);
+  const int P = w.y * blockDim.x + threadIdx.x;
+  if (P >= C.n) return;
+  float v = 0.0f;
+  for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) v = v + F.r[F.childP[q]];
+  C.bc[P] = v;
+  C.x[P] = 0.0f;
+}
+
+__global__ void k_prolong32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
+                               const SolveCtl* __restrict__ ctl) {
+  const int2 w = work[blockIdx.x];
+  if (!ctl[w.x].active) return;
+  const LevDesc& F = LEV(0, w.x);
+  const LevDesc& C = LEV(1, w.x);
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p >= F.n) return;
+  F.x[p] = F.x[p] + C.x[F.parentsP[p]];
+}
+
 __global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work, int color,
                        const SolveCtl* __restrict__ ctl) {
   const int2 w = work[blockIdx.x];
@@ -342,8 +423,6 @@ __global__ void k_prolong32(const LevDesc* __restrict__ levTab, int ns, int l, c
 // applies X with one dense product. Coarsest levels above kDense rows (reached only when
 // max_coarse_levels stops the hierarchy early) get 40 FP64 Gauss-Seidel sweeps instead.
 constexpr int kDense = 64;
-// levels of at most this many rows are smoothed inside the per-slot CTA of k_coarse_vcycle
-constexpr int kCtaRows = 2048;
 constexpr int kDenseLd = kDense + 1;
 struct DenseFactorSmem {
   double M[kDense][kDenseLd];
@@ -595,7 +674,13 @@ int Service::rebuild_tables() {
         d.childStart = l + 1 < nl ? L.childStart.p : nullptr;
         d.child = l + 1 < nl ? L.child.p : nullptr;
         d.colorRows = L.colorRows.p; d.colorStart = L.colorStart.p;
-        if (l == 0) { d.fr = L.fr.p; d.fp = L.fp.p; d.fq = L.fq.p; }
+        if (l == 0) {
+          d.fr = L.fr.p; d.fp = L.fp.p; d.fq = L.fq.p;
+          d.pmode = (nl > 1 && L.l0_valid) ? 1 : 0;
+          d.ellW = L.ellW;
+          d.perm = L.perm.p; d.inv = L.inv.p; d.ellCol = L.ellCol.p; d.ellAnb = L.ellAnb.p;
+          d.parentsP = L.parentsP.p; d.childP = L.childP.p;
+        }
       }
       lt[(size_t)l * ns + s] = d;
     }
@@ -611,7 +696,7 @@ int Service::rebuild_tables() {
     int g = 0;
     if (L > 0) {
       g = 1;
-      while (g < L && cases[q]->lev[g].n > kCtaRows) ++g;
+      while (g < L && cases[q]->lev[g].n > cta_rows) ++g;
     }
     hco[q] = L;
     hg[q] = g;
@@ -696,6 +781,7 @@ int Service::ensure_hierarchy(Case& c) {
       UFVM_CHECK(dalloc(L.fq, L.n));
     }
   }
+  if (c.n_levels > 1) UFVM_CHECK(build_l0(c));
   c.hierarchy_valid = true;
   tables_dirty = true;
   return UFVM_OK;
@@ -736,6 +822,52 @@ int Service::loop_end() {
   stream = main_stream;
   cudaGraph_t g = nullptr;
   UFVM_CUDA(cudaStreamEndCapture(bstream, &g));
+  return UFVM_OK;
+}
+
+// Level 0 of the FP32 V-cycle in colour-permuted ELL form (built once per hierarchy): rows
+// sorted by colour, natural order inside a colour (a stable counting sort on the host).
+int Service::build_l0(Case& c) {
+  Level& L = c.lev[0];
+  const int n = L.n, nnz = L.nnz;
+  if (!L.color_valid || c.n_levels < 2) { L.l0_valid = false; return UFVM_OK; }
+  std::vector<int> color(n), rp(n + 1), col(std::max(nnz, 1)), parents(n), cs(L.ncolor + 1), child(n);
+  UFVM_CUDA(cudaMemcpyAsync(color.data(), L.color.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  UFVM_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  if (nnz) UFVM_CUDA(cudaMemcpyAsync(col.data(), L.col.p, nnz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  UFVM_CUDA(cudaMemcpyAsync(parents.data(), L.parents.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  UFVM_CUDA(cudaMemcpyAsync(child.data(), L.child.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  UFVM_CUDA(cudaStreamSynchronize(stream));
+  std::vector<int> perm(n), inv(n), start(L.ncolor + 1, 0);
+  for (int i = 0; i < n; ++i) start[color[i] + 1]++;
+  for (int k = 0; k < L.ncolor; ++k) start[k + 1] += start[k];
+  if (start[L.ncolor] != n) { set_error("build_l0: colouring does not cover every row"); return UFVM_E_INVALID; }
+  {
+    std::vector<int> cur(start.begin(), start.end() - 1);
+    for (int i = 0; i < n; ++i) perm[cur[color[i]]++] = i;
+  }
+  for (int p = 0; p < n; ++p) inv[perm[p]] = p;
+  int W = 0;
+  for (int i = 0; i < n; ++i) W = std::max(W, rp[i + 1] - rp[i]);
+  std::vector<int> ell((size_t)W * n, -1), parP(n), chP(n);
+  for (int p = 0; p < n; ++p) {
+    const int i = perm[p];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) ell[(size_t)(k - rp[i]) * n + p] = inv[col[k]];
+    parP[p] = parents[i];
+  }
+  for (int q = 0; q < n; ++q) chP[q] = inv[child[q]];
+  // the colour ranges of the permuted storage are the colour starts of the natural colouring
+  for (int k = 0; k <= L.ncolor; ++k)
+    if (start[k] != L.h_colorStart[k]) { set_error("build_l0: colour ranges disagree"); return UFVM_E_INVALID; }
+  UFVM_CHECK(upload_vec(L.perm, perm, stream));
+  UFVM_CHECK(upload_vec(L.inv, inv, stream));
+  UFVM_CHECK(upload_vec(L.ellCol, ell, stream));
+  UFVM_CHECK(upload_vec(L.parentsP, parP, stream));
+  UFVM_CHECK(upload_vec(L.childP, chP, stream));
+  UFVM_CHECK(dalloc(L.ellAnb, std::max<size_t>((size_t)W * n, 1)));
+  UFVM_CUDA(cudaStreamSynchronize(stream));  // the host vectors above go out of scope
+  L.ellW = W;
+  L.l0_valid = true;
   return UFVM_OK;
 }
 
@@ -791,7 +923,7 @@ int Service::solve_p(bool g) {
   cudaGraphConditionalHandle h = 0;
   k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(pctl.p, ns);
   // FP32 copy of level 0 and FP64 Galerkin products, then their FP32 copies
-  k_lev_to32<<<nwrows[0], kBlock, 0, stream>>>(levTab.p, ns, 0, wrows[0].p, pctl.p);
+  k_l0_to32<<<nwrows[0], kBlock, 0, stream>>>(levTab.p, ns, wrows[0].p, pctl.p);
   for (int l = 0; l + 1 < Lmax; ++l) {
     k_galerkin_b<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l, wrows[l + 1].p, pctl.p);
     k_lev_to32<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l + 1, wrows[l + 1].p, pctl.p);
@@ -809,7 +941,8 @@ int Service::solve_p(bool g) {
         for (int q = 0; q < maxcol[l]; ++q) {
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
-          k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+          if (l == 0) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, wsm[0].p + smoff[0][c], c, pctl.p);
+          else k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
         }
   };
   // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
@@ -823,13 +956,19 @@ int Service::solve_p(bool g) {
     // large levels as grid-wide launches, the small ones per slot in one CTA
     for (int l = 0; l < maxg; ++l) {
       smooth(l, s.p_pre_sweep);
-      k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
-      k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
+      if (l == 0) {
+        k_res32_l0<<<nwnc[0], kBlock, 0, stream>>>(levTab.p, ns, wnc[0].p, pctl.p);
+        k_restrict32_l0<<<nwrc[0], kBlock, 0, stream>>>(levTab.p, ns, wrc[0].p, pctl.p);
+      } else {
+        k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+        k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
+      }
     }
     k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
                                              s.p_post_sweep, pctl.p);
     for (int l = maxg - 1; l >= 0; --l) {
-      k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+      if (l == 0) k_prolong32_l0<<<nwnc[0], kBlock, 0, stream>>>(levTab.p, ns, wnc[0].p, pctl.p);
+      else k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
       smooth(l, s.p_post_sweep);
     }
     if (s.p_krylov) {
@@ -1117,7 +1256,8 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
 // touched once per pass; neighbour gathers of x counted as cache hits). Units:
 //   0: one symmetric FP64 multicolour Gauss-Seidel sweep of every slot's level 0 (k_mc64,
 //      2 x colours launches): 2 x (40 B per row + 12 B per nonzero);
-//   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32): 2 x (24 B/row + 8 B/nz);
+//   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32_l0, colour-permuted ELL):
+//      2 x (16 B per row -- ac, bc, x written, x read once -- + 8 B per nonzero);
 //   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz.
 // The sweeps overwrite the slots' correction vectors, which the next assembly re-zeroes.
 int Service::profile(int kernel, int reps, double* ms, double* bytes) {
@@ -1139,7 +1279,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
         for (int q = 0; q < maxcol[0]; ++q) {
           const int c = pass == 0 ? q : maxcol[0] - 1 - q;
           if (smcnt[0][c] == 0) continue;
-          k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
+          k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, wsm[0].p + smoff[0][c], c, pctl.p);
         }
     } else {
       k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,
@@ -1176,7 +1316,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   cudaEventDestroy(b);
   *ms = t / reps;
   if (kernel == 0) *bytes = 2.0 * (40.0 * N + 12.0 * NNZ);
-  else if (kernel == 1) *bytes = 2.0 * (24.0 * N + 8.0 * NNZ);
+  else if (kernel == 1) *bytes = 2.0 * (16.0 * N + 8.0 * NNZ);
   else *bytes = 36.0 * N + 12.0 * NNZ;
   return UFVM_OK;
 }

@@ -17,6 +17,11 @@ struct LevDesc {
   const int *childStart, *child; // children in this level of each next-level row
   const int *colorRows, *colorStart;
   double *fr, *fp, *fq;          // level 0 only: FP64 flexible-CG vectors
+  // level 0 only: colour-permuted ELL storage of the FP32 arrays (pmode 1); ac, bc, x, r are
+  // then indexed by permuted position
+  int pmode, ellW;
+  const int *perm, *inv, *ellCol, *parentsP, *childP;
+  float* ellAnb;
 };
 
 // Per-slot control state of the batched linear solves (device resident).
@@ -86,10 +91,15 @@ struct Service {
   DArr<unsigned long long> loopcnt;
   unsigned long long loops_seen[2] = {0, 0};
 
+  // schedule: levels of at most cta_rows rows are smoothed inside the per-case CTA of the coarse
+  // V-cycle kernel, larger ones by grid-wide launches over all cases
+  int cta_rows = 2048;
+
   int rebuild_tables();
   BatchLaunch batch();
   bool needs_hierarchy(const Case& c) const;
   int ensure_hierarchy(Case& c);
+  int build_l0(Case& c);
   int loop_begin(int kind, cudaGraphConditionalHandle* h);
   int loop_end();
   int solve_u(bool g);

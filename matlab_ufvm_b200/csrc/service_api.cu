@@ -318,6 +318,15 @@ int ufvm_service_set_admit_interval(ufvm_service* h, int32_t steps) {
   return UFVM_OK;
 }
 
+int ufvm_service_set_schedule(ufvm_service* h, int32_t cta_rows) {
+  if (!h || cta_rows < 1) return UFVM_E_INVALID;
+  if (h->impl.svc.cta_rows != cta_rows) {
+    h->impl.svc.cta_rows = cta_rows;
+    h->impl.svc.tables_dirty = true;
+  }
+  return UFVM_OK;
+}
+
 int ufvm_service_stream(ufvm_service* h, void** stream) {
   if (!h || !stream) return UFVM_E_INVALID;
   *stream = (void*)h->impl.svc.stream;
