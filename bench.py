@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores (at most 64)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run for ncu: eager launches, warm-up only, then one roofline unit of the "
+                         "dominant kernel and one step inside cudaProfilerStart/Stop; prints the unit's bytes")
     return ap.parse_args()
 
 
@@ -302,9 +305,41 @@ def run_service(args, rank, ws, e2e: bool):
     return svc, out
 
 
+ROOF_KERNEL = (1, "k_mc32_l0 (FP32 multicolour Gauss-Seidel sweep of the V-cycle's level 0, "
+                  "colour-permuted ELL; one unit = both colours forward then backward over every case)")
+
+
+def main_profile(args):
+    """ncu target: the kernels of one unit of the roofline kernel and of one eager step."""
+    import torch
+    from matlab_ufvm_b200 import build as _b, ufvm
+    torch.cuda.set_device(0)
+    _b.build()
+    prebuild_meshes(range(1200))
+    settings = ufvm.fast_settings(base_spec(16))
+    settings.service_eager = 1
+    svc = ufvm.Service(settings, max_resident_cells=args.budget)
+    svc.set_schedule(8192)
+    feed = Feeder(svc, 0, 1)
+    feed.fill(0)
+    for _ in range(args.warmup * args.ticks):
+        nr, nq, nf = svc.step()
+        svc.poll()
+        feed.fill(nq)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    ms, by = svc.profile(ROOF_KERNEL[0], 1)
+    svc.step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_unit_bytes": by, "profile_unit_ms": ms, "resident": nr}), flush=True)
+    svc.close()
+    return 0
+
+
 def roofline(svc, peaks):
     """Dominant kernel, timed live on the resident batch."""
-    kernel_id, name = 1, "k_mc32 (FP32 multicolour Gauss-Seidel sweep, V-cycle level 0)"
+    kernel_id, name = ROOF_KERNEL
     ms, by = svc.profile(kernel_id, 20)
     achieved = by / (ms * 1e-3) / 1e9
     peak = peaks.get("hbm_gbs")
@@ -550,6 +585,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return main_reference(args)
+    if args.profile:
+        return main_profile(args)
     return main_ours(args)
 
 

@@ -218,7 +218,8 @@ int ufvm_service_release(ufvm_service* s, int64_t ticket);
  * U assembly, U solve, U correction, p assembly, AMG hierarchy builds, p solve, p correction --
  * then the number of U smoother sweeps, p V-cycles, steps, the service clock (ms), the ticks
  * replayed as a captured graph, the number of graph captures and the kernel launches executed by
- * the replayed graphs (loop bodies counted per execution). Writes min(n, 15) values. */
+ * the replayed graphs (loop bodies counted per execution), the current CTA threshold of the
+ * V-cycle and the number of completed autotuning passes. Writes min(n, 17) values. */
 int ufvm_service_stats(ufvm_service* s, double* out, int n);
 /* Tickets that finished (converged, stopped or failed) since the previous poll, oldest first:
  * writes min(capacity, pending) of them and their count; the rest stay for the next poll. */
@@ -229,7 +230,9 @@ int ufvm_service_poll(ufvm_service* s, int64_t* tickets, int64_t capacity, int64
 int ufvm_service_set_admit_interval(ufvm_service* s, int32_t steps);
 /* Launch schedule of the p solve's V-cycle: AMG levels of at most cta_rows rows are smoothed
  * by one thread block per case (all of a case's small levels in one launch), larger levels by
- * grid-wide launches over all cases (default 2048). Takes effect at the next step. */
+ * grid-wide launches over all cases. By default an autotuner picks cta_rows by timing the
+ * candidates 2048 .. 65536 on the live batch (re-tuned every 2000 steps); a positive value
+ * fixes the schedule, 0 hands it back to the autotuner. The schedule changes no result. */
 int ufvm_service_set_schedule(ufvm_service* s, int32_t cta_rows);
 /* The CUDA stream (cudaStream_t) on which the service issues all of its device work, so a
  * caller can order its own work or timing events after a step. No counterpart in the

@@ -307,11 +307,32 @@ __global__ void k_l0_to32(const LevDesc* __restrict__ levTab, int ns, const int2
   for (int k = 0; k < A.ellW; ++k) A.ellAnb[(size_t)k * A.n + p] = k < deg ? (float)A.anb64[k0 + k] : 0.0f;
 }
 
+// v - sum_k anb_k x_k over the row's entries in order. Up to kEllUnroll entries the column
+// and coefficient loads are all issued before the first neighbour gather.
+constexpr int kEllUnroll = 8;
 __device__ __forceinline__ float l0_row_sum(const LevDesc& A, int p, float v) {
-  for (int k = 0; k < A.ellW; ++k) {
-    const int c = A.ellCol[(size_t)k * A.n + p];
+  const int W = A.ellW;
+  const size_t n = (size_t)A.n;
+  if (W <= kEllUnroll) {
+    int c[kEllUnroll];
+    float a[kEllUnroll];
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k) {
+      c[k] = k < W ? A.ellCol[k * n + p] : -1;
+      a[k] = k < W ? A.ellAnb[k * n + p] : 0.0f;
+    }
+    float xv[kEllUnroll];
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? A.x[c[k]] : 0.0f;
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k)
+      if (c[k] >= 0) v = v - a[k] * xv[k];
+    return v;
+  }
+  for (int k = 0; k < W; ++k) {
+    const int c = A.ellCol[k * n + p];
     if (c < 0) break;
-    v = v - A.ellAnb[(size_t)k * A.n + p] * A.x[c];
+    v = v - A.ellAnb[k * n + p] * A.x[c];
   }
   return v;
 }

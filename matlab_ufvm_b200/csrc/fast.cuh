@@ -93,7 +93,8 @@ struct Service {
 
   // schedule: levels of at most cta_rows rows are smoothed inside the per-case CTA of the coarse
   // V-cycle kernel, larger ones by grid-wide launches over all cases
-  int cta_rows = 2048;
+  int cta_rows = 8192;
+  long long n_tunes = 0;
 
   int rebuild_tables();
   BatchLaunch batch();

@@ -45,6 +45,16 @@ struct ServiceImpl {
   // cannot be replayed from the captured graph, so admissions are gathered into few steps
   int admit_interval = 8;
   long long steps_since_admit = 1 << 30;
+  // schedule autotuner: times the candidate CTA thresholds of the V-cycle on the live batch
+  // (graph-replayed steps only; the first step after each switch, which re-captures the graph,
+  // is not timed), interleaved over two rounds, and keeps the fastest. The threshold does not
+  // change any result, only which launches run the small levels. Re-tunes every tune_every steps.
+  bool tune_on = true;
+  long long tune_every = 2000, next_tune = 24, steps = 0;
+  std::vector<int> tune_cand = {2048, 4096, 8192, 16384, 65536};
+  int tune_pos = -1, tune_in_cand = 0;  // position in the candidate sequence; steps at it
+  std::vector<double> tune_ms;
+  std::vector<int> tune_n;
   std::vector<long long> finished_unpolled;  // tickets finished since the last poll
   ~ServiceImpl() {
     for (auto& kv : rec)
@@ -102,6 +112,47 @@ static int admit(ServiceImpl& S) {
   }
   if (S.svc.cases.size() != before) S.steps_since_admit = 0;
   return UFVM_OK;
+}
+
+// One step of the schedule autotuner (called after every timed step).
+static void tune_step(ServiceImpl& S, double ms, bool graph_step) {
+  if (!S.tune_on) return;
+  const int nc = (int)S.tune_cand.size();
+  if (S.tune_pos < 0) {
+    if (S.steps < S.next_tune || S.svc.cases.size() < 2) return;
+    S.tune_ms.assign(nc, 0.0);
+    S.tune_n.assign(nc, 0);
+    S.tune_pos = 0;
+    S.tune_in_cand = 0;
+    S.svc.cta_rows = S.tune_cand[0];
+    S.svc.tables_dirty = true;
+    return;
+  }
+  const int cand = S.tune_pos % nc;
+  // step 0 at a candidate re-captures the graph; steps 1-2 are timed
+  if (S.tune_in_cand >= 1 && graph_step) {
+    S.tune_ms[cand] += ms;
+    S.tune_n[cand] += 1;
+  }
+  if (++S.tune_in_cand < 3) return;
+  S.tune_in_cand = 0;
+  if (++S.tune_pos < 2 * nc) {
+    S.svc.cta_rows = S.tune_cand[S.tune_pos % nc];
+    S.svc.tables_dirty = true;
+    return;
+  }
+  int best = -1;
+  double best_ms = 0;
+  for (int k = 0; k < nc; ++k)
+    if (S.tune_n[k] > 0 && (best < 0 || S.tune_ms[k] / S.tune_n[k] < best_ms)) {
+      best = k;
+      best_ms = S.tune_ms[k] / S.tune_n[k];
+    }
+  if (best >= 0) S.svc.cta_rows = S.tune_cand[best];
+  S.svc.tables_dirty = true;
+  S.tune_pos = -1;
+  S.next_tune = S.steps + S.tune_every;
+  ++S.svc.n_tunes;
 }
 
 }  // namespace ufvm
@@ -179,7 +230,9 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
   ServiceImpl& S = h->impl;
   Service& V = S.svc;
   UFVM_CHECK(admit(S));
+  ++S.steps;
   if (!V.cases.empty()) {
+    const long long graph_before = V.n_graph_ticks;
     UFVM_CUDA(cudaEventRecord(S.e0, V.stream));
     std::vector<double> res;
     std::vector<int> conv;
@@ -190,6 +243,7 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
     float ms = 0;
     UFVM_CUDA(cudaEventElapsedTime(&ms, S.e0, S.e1));
     S.clock_ms += ms;
+    tune_step(S, ms, V.n_graph_ticks != graph_before);
     std::vector<Case*> keep;
     std::vector<long long> keept;
     for (size_t q = 0; q < V.cases.size(); ++q) {
@@ -292,6 +346,8 @@ int ufvm_service_stats(ufvm_service* h, double* out, int n) {
   v.push_back((double)V.n_graph_ticks);
   v.push_back((double)V.n_captures);
   v.push_back((double)V.launches_total);
+  v.push_back((double)V.cta_rows);
+  v.push_back((double)V.n_tunes);
   for (int i = 0; i < n; ++i) out[i] = i < (int)v.size() ? v[i] : 0.0;
   return UFVM_OK;
 }
@@ -319,7 +375,14 @@ int ufvm_service_set_admit_interval(ufvm_service* h, int32_t steps) {
 }
 
 int ufvm_service_set_schedule(ufvm_service* h, int32_t cta_rows) {
-  if (!h || cta_rows < 1) return UFVM_E_INVALID;
+  if (!h || cta_rows < 0) return UFVM_E_INVALID;
+  if (cta_rows == 0) {  // hand the schedule back to the autotuner
+    h->impl.tune_on = true;
+    h->impl.next_tune = h->impl.steps;
+    return UFVM_OK;
+  }
+  h->impl.tune_on = false;
+  h->impl.tune_pos = -1;
   if (h->impl.svc.cta_rows != cta_rows) {
     h->impl.svc.cta_rows = cta_rows;
     h->impl.svc.tables_dirty = true;
