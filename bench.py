@@ -195,32 +195,18 @@ def barrier(ws):
 
 
 def reduce_max(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from matlab_ufvm_b200 import sharding
+    return sharding.reduce_max(x)
 
 
 def reduce_sum(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from matlab_ufvm_b200 import sharding
+    return sharding.reduce_sum(x)
 
 
 def gather_list(xs, ws):
-    if ws == 1:
-        return list(xs)
-    import torch.distributed as dist
-    out = [None] * ws
-    dist.all_gather_object(out, list(xs))
-    return [v for part in out for v in part]
+    from matlab_ufvm_b200 import sharding
+    return sharding.gather(xs)
 
 
 # ------------------------------------------------------------------ the service run
@@ -235,7 +221,8 @@ class Feeder:
         self.h2d = 0
 
     def next_index(self):
-        i = self.rank + self.ws * self.k
+        from matlab_ufvm_b200 import sharding
+        i = sharding.stream_index(self.rank, self.ws, self.k)
         self.k += 1
         return i
 
@@ -518,7 +505,8 @@ def main_ours(args):
     from matlab_ufvm_b200 import build as _b
     _b.build()
     # meshes for the first cases of this rank's share (the rest are built on demand)
-    prebuild_meshes([rank + ws * k for k in range(1200)])
+    from matlab_ufvm_b200 import sharding
+    prebuild_meshes([sharding.stream_index(rank, ws, k) for k in range(1200)])
     peaks = load_peaks()
     svc, res = run_service(args, rank, ws, e2e=False)
     roof = roofline(svc, peaks) if rank == 0 else None

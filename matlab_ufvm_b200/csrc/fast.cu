@@ -1,21 +1,22 @@
 // fast.cu -- the batched steady-case service (many cases, one launch per stage).
 //
-// Linear solves (new in this build, declared deviations from the reference's sequential
-// smoothers; the SIMPLE stages themselves are the reference's, shared with the plain path):
+// Linear solves (declared deviations from the reference's sequential smoothers; the SIMPLE
+// stages themselves are the reference's, shared with the plain path):
 //   U : multicolour symmetric Gauss-Seidel in FP64 with the reference's stopping rule
 //       (solve/cfdSolveAlgebraicSystem.m:38-46: at most u_n_iter sweeps, stop once
 //       sum|r|/N <= rrf * initial), evaluated per case on the device.
-//   p : FP32 AMG V-cycles on the correction equation inside FP64 iterative refinement:
-//       r = b - A x in FP64, e ~ A^-1 r by one FP32 V-cycle (multicolour GS smoothing, FP32
-//       restriction / prolongation by the agglomeration maps, FP64 dense coarsest solve),
-//       x += e in FP64; cycles stop per case on the reference's rule (cfdApplyAMG.m:27-52:
-//       at most p_max_cycles, stop once sum|r| <= termination * initial).
+//   p : FP64 flexible CG preconditioned by one FP32 agglomeration-AMG V-cycle (multicolour GS
+//       smoothing, FP32 restriction / prolongation by the agglomeration maps, FP64 coarsest
+//       solution operator); the residual, search directions and the update stay FP64, and
+//       iterations stop per case on the reference's rule (cfdApplyAMG.m:27-52: at most
+//       p_max_cycles, stop once sum|r| <= termination * initial). p_krylov 0 gives plain FP64
+//       iterative refinement (x += V(r)) instead.
 // The agglomeration maps are the reference's (exact seed agglomeration of the assembled p
 // matrix) built on a case's first p solve and reused; the Galerkin coarse operators are
-// recomputed in FP64 from the current matrix at every p solve.
-//
-// Roofline (FP32 MCGS half-sweep, per row): 4 ac + 4 bc + 4 x(r) + 4 x(w) + 4 colorRows
-// + 8 rowptr + nnz_row * (4 anb + 4 col + 4 x gather).
+// recomputed in FP64 from the current matrix at every p solve. Level 0 of the V-cycle is
+// stored colour-permuted in ELL form; levels up to cta_rows rows run one CTA per case.
+// A step without hierarchy builds is captured once and replayed as a CUDA graph whose solve
+// loops are conditional WHILE nodes ended on the device.
 #include "fast.cuh"
 
 namespace ufvm {

@@ -40,9 +40,13 @@ def test_service_result_same_alone_and_in_mix(ufvm_mod):
              case.cavity_case(6, nu=0.002, dim=3, quirks=case.QUIRKS_CONVERGING)]
     alone = [_run_alone(ufvm_mod, s) for s in specs]
     svc = ufvm_mod.Service(ufvm_mod.fast_settings(specs[0]), max_resident_cells=600)  # forces queueing
-    ts = [svc.submit(s, 3000) for s in specs]
+    ts = [svc.submit(s, 3000) for s in specs[:2]]
     nr, nq, nf = svc.step()
-    assert nq >= 1  # the third case waits for room
+    for _ in range(4):
+        svc.step()
+    ts.append(svc.submit(specs[2], 3000))  # arrives while the others are on the GPU
+    nr, nq, nf = svc.step()
+    assert nq >= 1  # and waits for room
     svc.run()
     for t, (st, U, p, md) in zip(ts, alone):
         s2 = svc.status(t)
