@@ -302,7 +302,7 @@ def main_profile(args):
     from matlab_ufvm_b200 import build as _b, ufvm
     torch.cuda.set_device(0)
     _b.build()
-    prebuild_meshes(range(1200))
+    # meshes are built on demand in this process (no worker pool under the profiler)
     settings = ufvm.fast_settings(base_spec(16))
     settings.service_eager = 1
     svc = ufvm.Service(settings, max_resident_cells=args.budget)

@@ -406,8 +406,9 @@ void free_level(Level& L, bool keep_matrix) {
   dfree(L.fwdStart); dfree(L.bwdRows); dfree(L.bwdStart); dfree(L.color); dfree(L.colorRows); dfree(L.colorStart);
   dfree(L.childStart); dfree(L.child); dfree(L.ac32); dfree(L.anb32); dfree(L.bc32); dfree(L.dphi32); dfree(L.r32);
   dfree(L.fr); dfree(L.fp); dfree(L.fq);
-  dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.ellAnb);
-  L.l0_valid = false;
+  dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.childStartP);
+  dfree(L.ellAnb);
+  L.ell_valid = false;
   L.sched_valid = false;
   L.color_valid = false;
 }

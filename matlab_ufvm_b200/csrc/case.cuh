@@ -49,12 +49,14 @@ struct Level {
   // FP64 flexible-CG vectors of the level-0 refinement (residual, search direction, A times
   // search direction)
   DArr<double> fr, fp, fq;
-  // level 0 of the batched service's FP32 V-cycle in colour-permuted ELL form: position p holds
-  // row perm[p] (colour-major, natural order inside a colour), inv is the inverse map, entry k
-  // of row p sits at [k * n + p] (column as a permuted index, -1 past the row's end)
-  bool l0_valid = false;
+  // the batched service's FP32 V-cycle stores every level but the coarsest colour-permuted in
+  // ELL form: position p holds row perm[p] (colour-major, natural order inside a colour), inv
+  // is the inverse map, entry k of row p sits at [k * n + p] (column as a position, -1 past
+  // the row's end); parentsP maps positions to the next level's storage indices, and
+  // childStartP / childP list each next-level storage index's children as positions
+  bool ell_valid = false;
   int ellW = 0;
-  DArr<int> perm, inv, ellCol, parentsP, childP;
+  DArr<int> perm, inv, ellCol, parentsP, childP, childStartP;
   DArr<float> ellAnb;
 };
 

@@ -247,17 +247,6 @@ __global__ void k_set_active(SolveCtl* ctl, int ns) {
 }
 
 // ---------------------------------------------------------------- FP32 AMG kernels
-__global__ void k_lev_to32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
-                           const SolveCtl* __restrict__ ctl) {
-  const int2 w = work[blockIdx.x];
-  if (!ctl[w.x].active) return;
-  const LevDesc& A = LEV(l, w.x);
-  const int i = w.y * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
-  A.ac[i] = (float)A.ac64[i];
-  for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) A.anb[k] = (float)A.anb64[k];
-}
-
 // Galerkin by summation from level l into level l+1 (assembleAgglomeratedLHS.m:16-30 order)
 __global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
                              const SolveCtl* __restrict__ ctl) {
@@ -287,15 +276,20 @@ __global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, 
   C.ac64[P] = AC;
 }
 
-// ---- level 0 of the V-cycle in colour-permuted ELL storage (pmode 1). Rows of one colour
-// are contiguous, so the row arrays are read with unit stride and every entry's column and
-// coefficient are coalesced across the warp; the only dependent load is the neighbour x.
-// Each row keeps the CSR (cconn) order of its entries.
-__global__ void k_l0_to32(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
-                          const SolveCtl* __restrict__ ctl) {
+// ---- FP32 levels of the V-cycle. Every level except a case's coarsest is stored colour-
+// permuted in ELL form (pmode 1): position p holds row perm[p], rows of one colour are
+// contiguous, entry k of position p sits at [k * n + p] with its column as a position. The row
+// arrays are then read with unit stride, every entry's column and coefficient are coalesced
+// across the warp, and the only dependent load is the neighbour x. Each row keeps the CSR
+// (cconn) order of its entries. A level in natural CSR form (pmode 0) is the coarsest level,
+// or level 0 of a case without a hierarchy.
+
+// FP32 copy of a level's FP64 matrix in its storage form (every p solve)
+__global__ void k_lev_to32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
+                           const SolveCtl* __restrict__ ctl) {
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
-  const LevDesc& A = LEV(0, w.x);
+  const LevDesc& A = LEV(l, w.x);
   const int p = w.y * blockDim.x + threadIdx.x;
   if (p >= A.n) return;
   if (!A.pmode) {
@@ -308,10 +302,14 @@ __global__ void k_l0_to32(const LevDesc* __restrict__ levTab, int ns, const int2
   for (int k = 0; k < A.ellW; ++k) A.ellAnb[(size_t)k * A.n + p] = k < deg ? (float)A.anb64[k0 + k] : 0.0f;
 }
 
-// v - sum_k anb_k x_k over the row's entries in order. Up to kEllUnroll entries the column
-// and coefficient loads are all issued before the first neighbour gather.
+// v - sum_k anb_k x_k over the row's entries in order. In ELL form and up to kEllUnroll
+// entries, the column and coefficient loads are all issued before the first neighbour gather.
 constexpr int kEllUnroll = 8;
-__device__ __forceinline__ float l0_row_sum(const LevDesc& A, int p, float v) {
+__device__ __forceinline__ float row_sum32(const LevDesc& A, int p, float v) {
+  if (!A.pmode) {
+    for (int k = A.rowptr[p]; k < A.rowptr[p + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
+    return v;
+  }
   const int W = A.ellW;
   const size_t n = (size_t)A.n;
   if (W <= kEllUnroll) {
@@ -338,52 +336,33 @@ __device__ __forceinline__ float l0_row_sum(const LevDesc& A, int p, float v) {
   return v;
 }
 
-__global__ void k_mc32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work, int color,
-                          const SolveCtl* __restrict__ ctl) {
-  const int2 w = work[blockIdx.x];
-  if (!ctl[w.x].active) return;
-  const LevDesc& A = LEV(0, w.x);
-  if (color >= A.ncolor) return;
-  const int s0 = A.colorStart[color], cnt = A.colorStart[color + 1] - s0;
-  const int t = w.y * blockDim.x + threadIdx.x;
-  if (t >= cnt) return;
-  const int p = s0 + t;
-  A.x[p] = l0_row_sum(A, p, A.bc[p]) / A.ac[p];
+// storage index of the t-th row of colour c
+__device__ __forceinline__ int color_row(const LevDesc& A, int c, int t) {
+  const int q = A.colorStart[c] + t;
+  return A.pmode ? q : A.colorRows[q];
 }
 
-__global__ void k_res32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
-                           const SolveCtl* __restrict__ ctl) {
-  const int2 w = work[blockIdx.x];
-  if (!ctl[w.x].active) return;
-  const LevDesc& A = LEV(0, w.x);
-  const int p = w.y * blockDim.x + threadIdx.x;
-  if (p >= A.n) return;
-  A.r[p] = l0_row_sum(A, p, A.bc[p] - A.ac[p] * A.x[p]);
+// one Gauss-Seidel update of row (storage index) p
+__device__ __forceinline__ void gs_row32(const LevDesc& A, int p) { A.x[p] = row_sum32(A, p, A.bc[p]) / A.ac[p]; }
+
+__device__ __forceinline__ void res_row32(const LevDesc& A, int p) {
+  A.r[p] = row_sum32(A, p, A.bc[p] - A.ac[p] * A.x[p]);
 }
 
-__global__ void k_restrict32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
-                                const SolveCtl* __restrict__ ctl) {
-  const int2 w = work[blockIdx.x];
-  if (!ctl[w.x].active) return;
-  const LevDesc& F = LEV(0, w.x);
-  const LevDesc& C = LEV(1, w.x);
-  const int P = w.y * blockDim.x + threadIdx.x;
-  if (P >= C.n) return;
+// restriction into coarse storage index P of the next level (children in their original order)
+__device__ __forceinline__ void restrict_row32(const LevDesc& F, const LevDesc& C, int P) {
   float v = 0.0f;
-  for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) v = v + F.r[F.childP[q]];
+  if (F.pmode) {
+    for (int q = F.childStartP[P]; q < F.childStartP[P + 1]; ++q) v = v + F.r[F.childP[q]];
+  } else {
+    for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) v = v + F.r[F.child[q]];
+  }
   C.bc[P] = v;
   C.x[P] = 0.0f;
 }
 
-__global__ void k_prolong32_l0(const LevDesc* __restrict__ levTab, int ns, const int2* __restrict__ work,
-                               const SolveCtl* __restrict__ ctl) {
-  const int2 w = work[blockIdx.x];
-  if (!ctl[w.x].active) return;
-  const LevDesc& F = LEV(0, w.x);
-  const LevDesc& C = LEV(1, w.x);
-  const int p = w.y * blockDim.x + threadIdx.x;
-  if (p >= F.n) return;
-  F.x[p] = F.x[p] + C.x[F.parentsP[p]];
+__device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C, int p) {
+  F.x[p] = F.x[p] + C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
 }
 
 __global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work, int color,
@@ -392,13 +371,9 @@ __global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const 
   if (!ctl[w.x].active) return;
   const LevDesc& A = LEV(l, w.x);
   if (color >= A.ncolor) return;
-  const int s0 = A.colorStart[color], cnt = A.colorStart[color + 1] - s0;
   const int t = w.y * blockDim.x + threadIdx.x;
-  if (t >= cnt) return;
-  const int i = A.colorRows[s0 + t];
-  float v = A.bc[i];
-  for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
-  A.x[i] = v / A.ac[i];
+  if (t >= A.colorStart[color + 1] - A.colorStart[color]) return;
+  gs_row32(A, color_row(A, color, t));
 }
 
 __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
@@ -406,11 +381,8 @@ __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& A = LEV(l, w.x);
-  const int i = w.y * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
-  float v = A.bc[i] - A.ac[i] * A.x[i];
-  for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
-  A.r[i] = v;
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p < A.n) res_row32(A, p);
 }
 
 __global__ void k_restrict32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
@@ -420,11 +392,7 @@ __global__ void k_restrict32(const LevDesc* __restrict__ levTab, int ns, int l, 
   const LevDesc& F = LEV(l, w.x);
   const LevDesc& C = LEV(l + 1, w.x);
   const int P = w.y * blockDim.x + threadIdx.x;
-  if (P >= C.n) return;
-  float v = 0.0f;
-  for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) v = v + F.r[F.child[q]];
-  C.bc[P] = v;
-  C.x[P] = 0.0f;
+  if (P < C.n) restrict_row32(F, C, P);
 }
 
 __global__ void k_prolong32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
@@ -433,9 +401,8 @@ __global__ void k_prolong32(const LevDesc* __restrict__ levTab, int ns, int l, c
   if (!ctl[w.x].active) return;
   const LevDesc& F = LEV(l, w.x);
   const LevDesc& C = LEV(l + 1, w.x);
-  const int i = w.y * blockDim.x + threadIdx.x;
-  if (i >= F.n) return;
-  F.x[i] = F.x[i] + C.x[F.parents[i]];
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p < F.n) prolong_row32(F, C, p);
 }
 
 // Coarsest level of each slot (at most kDense rows): its FP64 solution operator X, with
@@ -560,13 +527,8 @@ __device__ void smooth_cta(const LevDesc& A, int sweeps) {
     for (int pass = 0; pass < 2; ++pass)
       for (int q = 0; q < A.ncolor; ++q) {
         const int c = pass == 0 ? q : A.ncolor - 1 - q;
-        const int s0 = A.colorStart[c], s1 = A.colorStart[c + 1];
-        for (int t = s0 + threadIdx.x; t < s1; t += blockDim.x) {
-          const int i = A.colorRows[t];
-          float v = A.bc[i];
-          for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
-          A.x[i] = v / A.ac[i];
-        }
+        const int cnt = A.colorStart[c + 1] - A.colorStart[c];
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) gs_row32(A, color_row(A, c, t));
         __syncthreads();
       }
 }
@@ -587,25 +549,16 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle(const LevDesc* __restric
     const LevDesc& A = LEV(l, s);
     const LevDesc& C = LEV(l + 1, s);
     smooth_cta(A, pre);
-    for (int i = threadIdx.x; i < A.n; i += blockDim.x) {
-      float v = A.bc[i] - A.ac[i] * A.x[i];
-      for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
-      A.r[i] = v;
-    }
+    for (int p = threadIdx.x; p < A.n; p += blockDim.x) res_row32(A, p);
     __syncthreads();
-    for (int P = threadIdx.x; P < C.n; P += blockDim.x) {
-      float v = 0.0f;
-      for (int q = A.childStart[P]; q < A.childStart[P + 1]; ++q) v = v + A.r[A.child[q]];
-      C.bc[P] = v;
-      C.x[P] = 0.0f;
-    }
+    for (int P = threadIdx.x; P < C.n; P += blockDim.x) restrict_row32(A, C, P);
     __syncthreads();
   }
   coarse_apply_cta(LEV(L, s), cinv + (size_t)s * kDense * kDense);
   for (int l = L - 1; l >= g; --l) {
     const LevDesc& A = LEV(l, s);
     const LevDesc& C = LEV(l + 1, s);
-    for (int i = threadIdx.x; i < A.n; i += blockDim.x) A.x[i] = A.x[i] + C.x[A.parents[i]];
+    for (int p = threadIdx.x; p < A.n; p += blockDim.x) prolong_row32(A, C, p);
     __syncthreads();
     smooth_cta(A, post);
   }
@@ -696,12 +649,12 @@ int Service::rebuild_tables() {
         d.childStart = l + 1 < nl ? L.childStart.p : nullptr;
         d.child = l + 1 < nl ? L.child.p : nullptr;
         d.colorRows = L.colorRows.p; d.colorStart = L.colorStart.p;
-        if (l == 0) {
-          d.fr = L.fr.p; d.fp = L.fp.p; d.fq = L.fq.p;
-          d.pmode = (nl > 1 && L.l0_valid) ? 1 : 0;
+        if (l == 0) { d.fr = L.fr.p; d.fp = L.fp.p; d.fq = L.fq.p; }
+        d.pmode = (l + 1 < nl && L.ell_valid) ? 1 : 0;
+        if (d.pmode) {
           d.ellW = L.ellW;
           d.perm = L.perm.p; d.inv = L.inv.p; d.ellCol = L.ellCol.p; d.ellAnb = L.ellAnb.p;
-          d.parentsP = L.parentsP.p; d.childP = L.childP.p;
+          d.parentsP = L.parentsP.p; d.childP = L.childP.p; d.childStartP = L.childStartP.p;
         }
       }
       lt[(size_t)l * ns + s] = d;
@@ -803,7 +756,7 @@ int Service::ensure_hierarchy(Case& c) {
       UFVM_CHECK(dalloc(L.fq, L.n));
     }
   }
-  if (c.n_levels > 1) UFVM_CHECK(build_l0(c));
+  if (c.n_levels > 1) UFVM_CHECK(build_ell(c));
   c.hierarchy_valid = true;
   tables_dirty = true;
   return UFVM_OK;
@@ -847,49 +800,75 @@ int Service::loop_end() {
   return UFVM_OK;
 }
 
-// Level 0 of the FP32 V-cycle in colour-permuted ELL form (built once per hierarchy): rows
-// sorted by colour, natural order inside a colour (a stable counting sort on the host).
-int Service::build_l0(Case& c) {
-  Level& L = c.lev[0];
-  const int n = L.n, nnz = L.nnz;
-  if (!L.color_valid || c.n_levels < 2) { L.l0_valid = false; return UFVM_OK; }
-  std::vector<int> color(n), rp(n + 1), col(std::max(nnz, 1)), parents(n), cs(L.ncolor + 1), child(n);
-  UFVM_CUDA(cudaMemcpyAsync(color.data(), L.color.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  UFVM_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  if (nnz) UFVM_CUDA(cudaMemcpyAsync(col.data(), L.col.p, nnz * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  UFVM_CUDA(cudaMemcpyAsync(parents.data(), L.parents.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  UFVM_CUDA(cudaMemcpyAsync(child.data(), L.child.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  UFVM_CUDA(cudaStreamSynchronize(stream));
-  std::vector<int> perm(n), inv(n), start(L.ncolor + 1, 0);
-  for (int i = 0; i < n; ++i) start[color[i] + 1]++;
-  for (int k = 0; k < L.ncolor; ++k) start[k + 1] += start[k];
-  if (start[L.ncolor] != n) { set_error("build_l0: colouring does not cover every row"); return UFVM_E_INVALID; }
-  {
+// Every level but the coarsest of the FP32 V-cycle in colour-permuted ELL form (built once
+// per hierarchy): rows sorted by colour, natural order inside a colour (a stable counting
+// sort on the host).
+int Service::build_ell(Case& c) {
+  const int nl = c.n_levels;
+  if (nl < 2) return UFVM_OK;
+  std::vector<std::vector<int>> perm(nl), inv(nl);
+  for (int l = 0; l + 1 < nl; ++l) {
+    Level& L = c.lev[l];
+    L.ell_valid = false;
+    if (!L.color_valid) { set_error("build_ell: level without a colouring"); return UFVM_E_INVALID; }
+    const int n = L.n;
+    std::vector<int> color(n);
+    UFVM_CUDA(cudaMemcpyAsync(color.data(), L.color.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    UFVM_CUDA(cudaStreamSynchronize(stream));
+    std::vector<int> start(L.ncolor + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      if (color[i] < 0 || color[i] >= L.ncolor) { set_error("build_ell: row without a colour"); return UFVM_E_INVALID; }
+      start[color[i] + 1]++;
+    }
+    for (int k = 0; k < L.ncolor; ++k) start[k + 1] += start[k];
+    for (int k = 0; k <= L.ncolor; ++k)
+      if (start[k] != L.h_colorStart[k]) { set_error("build_ell: colour ranges disagree"); return UFVM_E_INVALID; }
+    perm[l].resize(n);
+    inv[l].resize(n);
     std::vector<int> cur(start.begin(), start.end() - 1);
-    for (int i = 0; i < n; ++i) perm[cur[color[i]]++] = i;
+    for (int i = 0; i < n; ++i) perm[l][cur[color[i]]++] = i;
+    for (int q = 0; q < n; ++q) inv[l][perm[l][q]] = q;
   }
-  for (int p = 0; p < n; ++p) inv[perm[p]] = p;
-  int W = 0;
-  for (int i = 0; i < n; ++i) W = std::max(W, rp[i + 1] - rp[i]);
-  std::vector<int> ell((size_t)W * n, -1), parP(n), chP(n);
-  for (int p = 0; p < n; ++p) {
-    const int i = perm[p];
-    for (int k = rp[i]; k < rp[i + 1]; ++k) ell[(size_t)(k - rp[i]) * n + p] = inv[col[k]];
-    parP[p] = parents[i];
+  for (int l = 0; l + 1 < nl; ++l) {
+    Level& L = c.lev[l];
+    const Level& C = c.lev[l + 1];
+    const bool cperm = l + 2 < nl;  // the next level is permuted too (it is not the coarsest)
+    const int n = L.n, nnz = L.nnz, nc = C.n;
+    std::vector<int> rp(n + 1), col(std::max(nnz, 1)), parents(n), cs(nc + 1), child(n);
+    UFVM_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (nnz) UFVM_CUDA(cudaMemcpyAsync(col.data(), L.col.p, nnz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    UFVM_CUDA(cudaMemcpyAsync(parents.data(), L.parents.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    UFVM_CUDA(cudaMemcpyAsync(cs.data(), L.childStart.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    UFVM_CUDA(cudaMemcpyAsync(child.data(), L.child.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    UFVM_CUDA(cudaStreamSynchronize(stream));
+    const std::vector<int>& P = perm[l];
+    const std::vector<int>& I = inv[l];
+    int W = 0;
+    for (int i = 0; i < n; ++i) W = std::max(W, rp[i + 1] - rp[i]);
+    std::vector<int> ell((size_t)W * n, -1), parP(n), chP, chS(nc + 1, 0);
+    chP.reserve(n);
+    for (int q = 0; q < n; ++q) {
+      const int i = P[q];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) ell[(size_t)(k - rp[i]) * n + q] = I[col[k]];
+      parP[q] = cperm ? inv[l + 1][parents[i]] : parents[i];
+    }
+    for (int Q = 0; Q < nc; ++Q) {
+      const int Pn = cperm ? perm[l + 1][Q] : Q;
+      for (int k = cs[Pn]; k < cs[Pn + 1]; ++k) chP.push_back(I[child[k]]);
+      chS[Q + 1] = (int)chP.size();
+    }
+    if ((int)chP.size() != n) { set_error("build_ell: children do not cover the level"); return UFVM_E_INVALID; }
+    UFVM_CHECK(upload_vec(L.perm, P, stream));
+    UFVM_CHECK(upload_vec(L.inv, I, stream));
+    UFVM_CHECK(upload_vec(L.ellCol, ell, stream));
+    UFVM_CHECK(upload_vec(L.parentsP, parP, stream));
+    UFVM_CHECK(upload_vec(L.childP, chP, stream));
+    UFVM_CHECK(upload_vec(L.childStartP, chS, stream));
+    UFVM_CHECK(dalloc(L.ellAnb, std::max<size_t>((size_t)W * n, 1)));
+    UFVM_CUDA(cudaStreamSynchronize(stream));  // the host vectors above go out of scope
+    L.ellW = W;
+    L.ell_valid = true;
   }
-  for (int q = 0; q < n; ++q) chP[q] = inv[child[q]];
-  // the colour ranges of the permuted storage are the colour starts of the natural colouring
-  for (int k = 0; k <= L.ncolor; ++k)
-    if (start[k] != L.h_colorStart[k]) { set_error("build_l0: colour ranges disagree"); return UFVM_E_INVALID; }
-  UFVM_CHECK(upload_vec(L.perm, perm, stream));
-  UFVM_CHECK(upload_vec(L.inv, inv, stream));
-  UFVM_CHECK(upload_vec(L.ellCol, ell, stream));
-  UFVM_CHECK(upload_vec(L.parentsP, parP, stream));
-  UFVM_CHECK(upload_vec(L.childP, chP, stream));
-  UFVM_CHECK(dalloc(L.ellAnb, std::max<size_t>((size_t)W * n, 1)));
-  UFVM_CUDA(cudaStreamSynchronize(stream));  // the host vectors above go out of scope
-  L.ellW = W;
-  L.l0_valid = true;
   return UFVM_OK;
 }
 
@@ -945,7 +924,7 @@ int Service::solve_p(bool g) {
   cudaGraphConditionalHandle h = 0;
   k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(pctl.p, ns);
   // FP32 copy of level 0 and FP64 Galerkin products, then their FP32 copies
-  k_l0_to32<<<nwrows[0], kBlock, 0, stream>>>(levTab.p, ns, wrows[0].p, pctl.p);
+  k_lev_to32<<<nwrows[0], kBlock, 0, stream>>>(levTab.p, ns, 0, wrows[0].p, pctl.p);
   for (int l = 0; l + 1 < Lmax; ++l) {
     k_galerkin_b<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l, wrows[l + 1].p, pctl.p);
     k_lev_to32<<<nwrows[l + 1], kBlock, 0, stream>>>(levTab.p, ns, l + 1, wrows[l + 1].p, pctl.p);
@@ -963,8 +942,7 @@ int Service::solve_p(bool g) {
         for (int q = 0; q < maxcol[l]; ++q) {
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
-          if (l == 0) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, wsm[0].p + smoff[0][c], c, pctl.p);
-          else k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+          k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
         }
   };
   // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
@@ -978,19 +956,13 @@ int Service::solve_p(bool g) {
     // large levels as grid-wide launches, the small ones per slot in one CTA
     for (int l = 0; l < maxg; ++l) {
       smooth(l, s.p_pre_sweep);
-      if (l == 0) {
-        k_res32_l0<<<nwnc[0], kBlock, 0, stream>>>(levTab.p, ns, wnc[0].p, pctl.p);
-        k_restrict32_l0<<<nwrc[0], kBlock, 0, stream>>>(levTab.p, ns, wrc[0].p, pctl.p);
-      } else {
-        k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
-        k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
-      }
+      k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+      k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
     }
     k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
                                              s.p_post_sweep, pctl.p);
     for (int l = maxg - 1; l >= 0; --l) {
-      if (l == 0) k_prolong32_l0<<<nwnc[0], kBlock, 0, stream>>>(levTab.p, ns, wnc[0].p, pctl.p);
-      else k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+      k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
       smooth(l, s.p_post_sweep);
     }
     if (s.p_krylov) {
@@ -1278,7 +1250,7 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
 // touched once per pass; neighbour gathers of x counted as cache hits). Units:
 //   0: one symmetric FP64 multicolour Gauss-Seidel sweep of every slot's level 0 (k_mc64,
 //      2 x colours launches): 2 x (40 B per row + 12 B per nonzero);
-//   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32_l0, colour-permuted ELL):
+//   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32, colour-permuted ELL):
 //      2 x (16 B per row -- ac, bc, x written, x read once -- + 8 B per nonzero);
 //   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz.
 // The sweeps overwrite the slots' correction vectors, which the next assembly re-zeroes.
@@ -1301,7 +1273,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
         for (int q = 0; q < maxcol[0]; ++q) {
           const int c = pass == 0 ? q : maxcol[0] - 1 - q;
           if (smcnt[0][c] == 0) continue;
-          k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, wsm[0].p + smoff[0][c], c, pctl.p);
+          k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
         }
     } else {
       k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,

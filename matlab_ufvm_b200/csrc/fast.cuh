@@ -17,10 +17,10 @@ struct LevDesc {
   const int *childStart, *child; // children in this level of each next-level row
   const int *colorRows, *colorStart;
   double *fr, *fp, *fq;          // level 0 only: FP64 flexible-CG vectors
-  // level 0 only: colour-permuted ELL storage of the FP32 arrays (pmode 1); ac, bc, x, r are
-  // then indexed by permuted position
+  // colour-permuted ELL storage of the FP32 arrays (pmode 1, every level but the coarsest);
+  // ac, bc, x, r are then indexed by position
   int pmode, ellW;
-  const int *perm, *inv, *ellCol, *parentsP, *childP;
+  const int *perm, *inv, *ellCol, *parentsP, *childP, *childStartP;
   float* ellAnb;
 };
 
@@ -100,7 +100,7 @@ struct Service {
   BatchLaunch batch();
   bool needs_hierarchy(const Case& c) const;
   int ensure_hierarchy(Case& c);
-  int build_l0(Case& c);
+  int build_ell(Case& c);
   int loop_begin(int kind, cudaGraphConditionalHandle* h);
   int loop_end();
   int solve_u(bool g);
