@@ -407,7 +407,7 @@ void free_level(Level& L, bool keep_matrix) {
   dfree(L.childStart); dfree(L.child); dfree(L.ac32); dfree(L.anb32); dfree(L.bc32); dfree(L.dphi32); dfree(L.r32);
   dfree(L.fr); dfree(L.fp); dfree(L.fq);
   dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.childStartP);
-  dfree(L.ellAnb);
+  dfree(L.ellAnb); dfree(L.uAnb); dfree(L.uAc); dfree(L.uBc); dfree(L.uX);
   L.ell_valid = false;
   L.sched_valid = false;
   L.color_valid = false;

@@ -58,6 +58,7 @@ struct Level {
   int ellW = 0;
   DArr<int> perm, inv, ellCol, parentsP, childP, childStartP;
   DArr<float> ellAnb;
+  DArr<double> uAnb, uAc, uBc, uX;  // level 0: FP64 ELL copy of the momentum matrix (service U solve)
 };
 
 // Scratch buffers for matrix-level work (owned by a Case or by a stand-alone call).

@@ -23,22 +23,89 @@ namespace ufvm {
 
 #define LEV(l, s) levTab[(size_t)(l) * ns + (s)]
 
+// rows of ELL matrices with at most this many entries issue all their column and coefficient
+// loads before the first neighbour gather
+constexpr int kEllUnroll = 8;
+
 // ---------------------------------------------------------------- FP64 fine-level kernels
-__global__ void k_res64_abs(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
-                            const SolveCtl* __restrict__ ctl, double* part) {
+// ---- the FP64 U solve. A case whose level 0 has the colour-permuted ELL layout (pmode 1)
+// smooths an ELL copy of its momentum matrix (uAc, uBc, uAnb at [k * n + p], uX), made after
+// each assembly and scattered back into dphi after the solve; a case without it (its first
+// step, before its hierarchy exists) smooths the natural CSR matrix through the colour rows.
+// Either way each row is v = bc - sum anb x in cconn order, x = v / ac.
+__device__ __forceinline__ double urow_sum(const LevDesc& A, int p, double v) {
+  const int W = A.ellW;
+  const size_t n = (size_t)A.n;
+  if (W <= kEllUnroll) {
+    int c[kEllUnroll];
+    double a[kEllUnroll];
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k) {
+      c[k] = k < W ? A.ellCol[k * n + p] : -1;
+      a[k] = k < W ? A.uAnb[k * n + p] : 0.0;
+    }
+    double xv[kEllUnroll];
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? A.uX[c[k]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k)
+      if (c[k] >= 0) v = v - a[k] * xv[k];
+    return v;
+  }
+  for (int k = 0; k < W; ++k) {
+    const int c = A.ellCol[k * n + p];
+    if (c < 0) break;
+    v = v - A.uAnb[k * n + p] * A.uX[c];
+  }
+  return v;
+}
+
+__global__ void k_res64_abs(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                            const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double* part) {
   __shared__ double sh[32];
   const int2 w = work[blockIdx.x];
   const SlotDesc& S = slots[w.x];
+  const LevDesc& A = LEV(0, w.x);
   const int i = w.y * blockDim.x + threadIdx.x;
   double v = 0.0;
   if (i < S.m.Nc && ctl[w.x].active) {
-    const int* rp = S.m.rowptr;
-    double r = S.bc[i] - S.ac[i] * S.dphi[i];
-    for (int k = rp[i]; k < rp[i + 1]; ++k) r = r - S.anb[k] * S.dphi[S.m.col[k]];
-    v = fabs(r);
+    if (A.pmode) {
+      v = fabs(urow_sum(A, i, A.uBc[i] - A.uAc[i] * A.uX[i]));
+    } else {
+      const int* rp = S.m.rowptr;
+      double r = S.bc[i] - S.ac[i] * S.dphi[i];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) r = r - S.anb[k] * S.dphi[S.m.col[k]];
+      v = fabs(r);
+    }
   }
   v = block_reduce<0>(v, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// ELL copy of the just-assembled momentum matrix (pmode cases)
+__global__ void k_u_to_ell(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                           const int2* __restrict__ work) {
+  const int2 w = work[blockIdx.x];
+  const LevDesc& A = LEV(0, w.x);
+  if (!A.pmode) return;
+  const SlotDesc& S = slots[w.x];
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  const int i = A.perm[p], k0 = S.m.rowptr[i], deg = S.m.rowptr[i + 1] - k0;
+  A.uAc[p] = S.ac[i];
+  A.uBc[p] = S.bc[i];
+  A.uX[p] = S.dphi[i];
+  for (int k = 0; k < A.ellW; ++k) A.uAnb[(size_t)k * A.n + p] = k < deg ? S.anb[k0 + k] : 0.0;
+}
+
+__global__ void k_u_from_ell(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
+                             const int2* __restrict__ work) {
+  const int2 w = work[blockIdx.x];
+  const LevDesc& A = LEV(0, w.x);
+  if (!A.pmode) return;
+  const SlotDesc& S = slots[w.x];
+  const int p = w.y * blockDim.x + threadIdx.x;
+  if (p < A.n) S.dphi[A.perm[p]] = A.uX[p];
 }
 
 // r = b - A x (FP64) -> FP32 right-hand side of the correction; e = 0
@@ -173,6 +240,11 @@ __global__ void k_mc64(const SlotDesc* __restrict__ slots, const LevDesc* __rest
   const int s0 = A.colorStart[color], cnt = A.colorStart[color + 1] - s0;
   const int t = w.y * blockDim.x + threadIdx.x;
   if (t >= cnt) return;
+  if (A.pmode) {
+    const int p = s0 + t;
+    A.uX[p] = urow_sum(A, p, A.uBc[p]) / A.uAc[p];
+    return;
+  }
   const int i = A.colorRows[s0 + t];
   const int* rp = S.m.rowptr;
   double v = S.bc[i];
@@ -304,7 +376,6 @@ __global__ void k_lev_to32(const LevDesc* __restrict__ levTab, int ns, int l, co
 
 // v - sum_k anb_k x_k over the row's entries in order. In ELL form and up to kEllUnroll
 // entries, the column and coefficient loads are all issued before the first neighbour gather.
-constexpr int kEllUnroll = 8;
 __device__ __forceinline__ float row_sum32(const LevDesc& A, int p, float v) {
   if (!A.pmode) {
     for (int k = A.rowptr[p]; k < A.rowptr[p + 1]; ++k) v = v - A.anb[k] * A.x[A.col[k]];
@@ -655,6 +726,7 @@ int Service::rebuild_tables() {
           d.ellW = L.ellW;
           d.perm = L.perm.p; d.inv = L.inv.p; d.ellCol = L.ellCol.p; d.ellAnb = L.ellAnb.p;
           d.parentsP = L.parentsP.p; d.childP = L.childP.p; d.childStartP = L.childStartP.p;
+          if (l == 0) { d.uAnb = L.uAnb.p; d.uAc = L.uAc.p; d.uBc = L.uBc.p; d.uX = L.uX.p; }
         }
       }
       lt[(size_t)l * ns + s] = d;
@@ -865,6 +937,12 @@ int Service::build_ell(Case& c) {
     UFVM_CHECK(upload_vec(L.childP, chP, stream));
     UFVM_CHECK(upload_vec(L.childStartP, chS, stream));
     UFVM_CHECK(dalloc(L.ellAnb, std::max<size_t>((size_t)W * n, 1)));
+    if (l == 0) {  // FP64 ELL copy of the momentum matrix for the U solve
+      UFVM_CHECK(dalloc(L.uAnb, std::max<size_t>((size_t)W * n, 1)));
+      UFVM_CHECK(dalloc(L.uAc, n));
+      UFVM_CHECK(dalloc(L.uBc, n));
+      UFVM_CHECK(dalloc(L.uX, n));
+    }
     UFVM_CUDA(cudaStreamSynchronize(stream));  // the host vectors above go out of scope
     L.ellW = W;
     L.ell_valid = true;
@@ -876,9 +954,10 @@ int Service::solve_u(bool g) {
   const int ns = (int)cases.size();
   const ufvm_settings& s = S;
   cudaGraphConditionalHandle h = 0;
+  k_u_to_ell<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p);
   // the first residual is taken for every slot
   k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(uctl.p, ns);
-  k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, wc.p, uctl.p, part.p);
+  k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
   k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
   // (in a captured tick the while node starts from its default condition 1: a body whose
   // slots are all inactive does nothing and its k_ctrl ends the loop)
@@ -892,7 +971,7 @@ int Service::solve_u(bool g) {
         if (ucol_cnt[c] == 0) continue;
         k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
       }
-    k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, wc.p, uctl.p, part.p);
+    k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
     k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
     k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 0, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
                                   SCAL_U_R1, anyflag.p, g, h, loopcnt.p, 0);
@@ -903,18 +982,21 @@ int Service::solve_u(bool g) {
     UFVM_CHECK(loop_begin(0, &h));
     const int st = body();
     UFVM_CHECK(loop_end());
-    return st;
-  }
-  int any = 0;
-  for (int it = 0; it < s.u_n_iter; ++it) {
-    ++n_usweeps;
-    UFVM_CHECK(body());
-    if (it & 1) {
-      UFVM_CUDA(cudaMemcpyAsync(&any, anyflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-      UFVM_CUDA(cudaStreamSynchronize(stream));
-      if (!any) break;
+    UFVM_CHECK(st);
+  } else {
+    int any = 0;
+    for (int it = 0; it < s.u_n_iter; ++it) {
+      ++n_usweeps;
+      UFVM_CHECK(body());
+      if (it & 1) {
+        UFVM_CUDA(cudaMemcpyAsync(&any, anyflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        UFVM_CUDA(cudaStreamSynchronize(stream));
+        if (!any) break;
+      }
     }
   }
+  k_u_from_ell<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p);
+  UFVM_LAUNCH_CHECK();
   return UFVM_OK;
 }
 
@@ -1248,8 +1330,9 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
 // Times one kernel of the tick on the current resident batch, `reps` times after one warm-up,
 // and returns the average device time of one unit and its compulsory bytes (every array
 // touched once per pass; neighbour gathers of x counted as cache hits). Units:
-//   0: one symmetric FP64 multicolour Gauss-Seidel sweep of every slot's level 0 (k_mc64,
-//      2 x colours launches): 2 x (40 B per row + 12 B per nonzero);
+//   0: one symmetric FP64 multicolour Gauss-Seidel sweep of every slot's level 0 (k_mc64 on
+//      the ELL copy, 2 x colours launches): 2 x (32 B per row -- ac, bc, x written, x read
+//      once -- + 12 B per nonzero);
 //   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32, colour-permuted ELL):
 //      2 x (16 B per row -- ac, bc, x written, x read once -- + 8 B per nonzero);
 //   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz.
@@ -1260,6 +1343,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   if (tables_dirty) UFVM_CHECK(rebuild_tables());
   double N = 0, NNZ = 0;
   for (auto* c : cases) { N += c->M.Nc; NNZ += c->M.nnz; }
+  if (kernel == 0) k_u_to_ell<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p);
   auto unit = [&]() -> int {
     if (kernel == 0) {
       for (int pass = 0; pass < 2; ++pass)
@@ -1309,7 +1393,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   *ms = t / reps;
-  if (kernel == 0) *bytes = 2.0 * (40.0 * N + 12.0 * NNZ);
+  if (kernel == 0) *bytes = 2.0 * (32.0 * N + 12.0 * NNZ);
   else if (kernel == 1) *bytes = 2.0 * (16.0 * N + 8.0 * NNZ);
   else *bytes = 36.0 * N + 12.0 * NNZ;
   return UFVM_OK;

@@ -22,6 +22,7 @@ struct LevDesc {
   int pmode, ellW;
   const int *perm, *inv, *ellCol, *parentsP, *childP, *childStartP;
   float* ellAnb;
+  double *uAnb, *uAc, *uBc, *uX;  // level 0, pmode: FP64 ELL copy of the momentum matrix
 };
 
 // Per-slot control state of the batched linear solves (device resident).

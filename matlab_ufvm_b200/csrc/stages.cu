@@ -101,7 +101,7 @@ __device__ __forceinline__ void grad_ptrs(const FieldView& f, const double** phi
 
 // compute/cfdComputeGradientGauss0.m:28-80 (Q1: boundary value of component 1)
 template <int W>
-__global__ void k_grad_cells(const SlotDesc* __restrict__ slots, const int2* __restrict__ work) {
+__global__ void __launch_bounds__(kBlock, 3) k_grad_cells(const SlotDesc* __restrict__ slots, const int2* __restrict__ work) {
   constexpr int NC = W == G_U ? 3 : 1;
   SLOT_BEGIN(work);
   const int e = idx;
@@ -260,7 +260,7 @@ __device__ __forceinline__ void face_grad_corr(const MeshView& m, int fc, int o,
 
 // cfdAssembleEquation('U', comp): convection (upwind) + convection divergence, diffusion,
 // explicit stress, pressure gradient, false transient, URF, scaled residual, DU.
-__global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restrict__ slots,
+__global__ void __launch_bounds__(kBlock, 3) k_assemble_u(const SlotDesc* __restrict__ slots,
                                                        const int2* __restrict__ work, int comp, double* part) {
   __shared__ double sh[32];
   SLOT_BEGIN(work);
@@ -438,7 +438,7 @@ __global__ void k_du_boundary(const SlotDesc* __restrict__ slots, const int2* __
 }
 
 // ---------------------------------------------------------------- Rhie-Chow (cfdAssembleMdotTerm.m)
-__global__ void k_rhiechow(const SlotDesc* __restrict__ slots, const int2* __restrict__ work) {
+__global__ void __launch_bounds__(kBlock, 3) k_rhiechow(const SlotDesc* __restrict__ slots, const int2* __restrict__ work) {
   SLOT_BEGIN(work);
   const int fc = idx;
   if (fc >= m.F) return;
