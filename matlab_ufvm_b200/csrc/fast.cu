@@ -17,6 +17,8 @@
 // stored colour-permuted in ELL form; levels up to cta_rows rows run one CTA per case.
 // A step without hierarchy builds is captured once and replayed as a CUDA graph whose solve
 // loops are conditional WHILE nodes ended on the device.
+#include <algorithm>
+
 #include "fast.cuh"
 
 namespace ufvm {
@@ -436,15 +438,56 @@ __device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C
   F.x[p] = F.x[p] + C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
 }
 
-__global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work, int color,
-                       const SolveCtl* __restrict__ ctl) {
+// Two ELL rows at once: all column and coefficient loads of both rows are issued before the
+// neighbour gathers of either, doubling the loads each thread keeps in flight.
+__device__ __forceinline__ void row_sum32_x2(const LevDesc& A, int p0, float& v0, int p1, float& v1, bool two) {
+  const int W = A.ellW;
+  const size_t n = (size_t)A.n;
+  int c0[kEllUnroll], c1[kEllUnroll];
+  float a0[kEllUnroll], a1[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) {
+    c0[k] = k < W ? A.ellCol[k * n + p0] : -1;
+    a0[k] = k < W ? A.ellAnb[k * n + p0] : 0.0f;
+    c1[k] = (two && k < W) ? A.ellCol[k * n + p1] : -1;
+    a1[k] = (two && k < W) ? A.ellAnb[k * n + p1] : 0.0f;
+  }
+  float x0[kEllUnroll], x1[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) {
+    x0[k] = c0[k] >= 0 ? A.x[c0[k]] : 0.0f;
+    x1[k] = c1[k] >= 0 ? A.x[c1[k]] : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) {
+    if (c0[k] >= 0) v0 = v0 - a0[k] * x0[k];
+    if (c1[k] >= 0) v1 = v1 - a1[k] * x1[k];
+  }
+}
+
+// One colour of a Gauss-Seidel sweep. Launched with kBlock / 2 threads per (slot, block) work
+// item of kBlock rows: each thread updates rows t and t + kBlock / 2 of the item.
+__global__ void __launch_bounds__(kBlock / 2) k_mc32(const LevDesc* __restrict__ levTab, int ns, int l,
+                                                     const int2* __restrict__ work, int color,
+                                                     const SolveCtl* __restrict__ ctl) {
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& A = LEV(l, w.x);
   if (color >= A.ncolor) return;
-  const int t = w.y * blockDim.x + threadIdx.x;
-  if (t >= A.colorStart[color + 1] - A.colorStart[color]) return;
-  gs_row32(A, color_row(A, color, t));
+  const int cnt = A.colorStart[color + 1] - A.colorStart[color];
+  const int t0 = w.y * kBlock + threadIdx.x, t1 = t0 + kBlock / 2;
+  if (t0 >= cnt) return;
+  const bool two = t1 < cnt;
+  if (A.pmode && A.ellW <= kEllUnroll) {
+    const int p0 = A.colorStart[color] + t0, p1 = A.colorStart[color] + t1;
+    float v0 = A.bc[p0], v1 = two ? A.bc[p1] : 0.0f;
+    row_sum32_x2(A, p0, v0, p1, v1, two);
+    A.x[p0] = v0 / A.ac[p0];
+    if (two) A.x[p1] = v1 / A.ac[p1];
+    return;
+  }
+  gs_row32(A, color_row(A, color, t0));
+  if (two) gs_row32(A, color_row(A, color, t1));
 }
 
 __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
@@ -609,11 +652,12 @@ __device__ void smooth_cta(const LevDesc& A, int sweeps) {
 // Descend with pre-smoothing, residual and restriction; apply the coarsest operator; ascend
 // with prolongation and post-smoothing. A slot whose coarsest level is 0 gets its direct solve
 // on level 0 here.
-__global__ void __launch_bounds__(1024) k_coarse_vcycle(const LevDesc* __restrict__ levTab, int ns,
+__global__ void __launch_bounds__(1024, 2) k_coarse_vcycle(const LevDesc* __restrict__ levTab, int ns,
                                                         const int* __restrict__ coarsest,
                                                         const int* __restrict__ gstart, const double* __restrict__ cinv,
-                                                        int pre, int post, const SolveCtl* __restrict__ ctl) {
-  const int s = blockIdx.x;
+                                                        int pre, int post, const SolveCtl* __restrict__ ctl,
+                                                        const int* __restrict__ order) {
+  const int s = order[blockIdx.x];
   if (!ctl[s].active) return;
   const int L = coarsest[s], g = gstart[s];
   for (int l = g; l < L; ++l) {
@@ -751,6 +795,15 @@ int Service::rebuild_tables() {
   }
   UFVM_CHECK(upload_vec(dcoarsest, hco, stream));
   UFVM_CHECK(upload_vec(dgstart, hg, stream));
+  {  // CTA order of the coarse V-cycle: the cases with the most rows below the grid levels first
+    std::vector<long long> work_rows(ns, 0);
+    for (int q = 0; q < ns; ++q)
+      for (int l = hg[q]; l <= hco[q]; ++l) work_rows[q] += cases[q]->lev[l].n;
+    std::vector<int> order(ns);
+    for (int q = 0; q < ns; ++q) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work_rows[a] > work_rows[b]; });
+    UFVM_CHECK(upload_vec(dcta_order, order, stream));
+  }
   UFVM_CHECK(dalloc(cinv, (size_t)ns * kDense * kDense));
   for (int l = 0; l < Lmax; ++l) {
     build_list(ns, [&](int q) { return l < nlev(q) ? cases[q]->lev[l].n : 0; }, v, nullptr, nullptr);
@@ -1024,7 +1077,7 @@ int Service::solve_p(bool g) {
         for (int q = 0; q < maxcol[l]; ++q) {
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
-          k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+          k_mc32<<<smcnt[l][c], kBlock / 2, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
         }
   };
   // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
@@ -1042,7 +1095,7 @@ int Service::solve_p(bool g) {
       k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
     }
     k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
-                                             s.p_post_sweep, pctl.p);
+                                             s.p_post_sweep, pctl.p, dcta_order.p);
     for (int l = maxg - 1; l >= 0; --l) {
       k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
       smooth(l, s.p_post_sweep);
@@ -1357,7 +1410,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
         for (int q = 0; q < maxcol[0]; ++q) {
           const int c = pass == 0 ? q : maxcol[0] - 1 - q;
           if (smcnt[0][c] == 0) continue;
-          k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
+          k_mc32<<<smcnt[0][c], kBlock / 2, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
         }
     } else {
       k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,
@@ -1424,7 +1477,7 @@ Service::~Service() {
   for (auto& a : wsm) dfree(a);
   for (auto& a : wnc) dfree(a);
   for (auto& a : wrc) dfree(a);
-  dfree(dcoarsest); dfree(dgstart); dfree(cinv);
+  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order);
   lin.release();
   for (auto e : evpool) destroy_check(cudaEventDestroy(e), "cudaEventDestroy");
   if (bstream) destroy_check(cudaStreamDestroy(bstream), "cudaStreamDestroy");

@@ -62,6 +62,7 @@ struct Service {
   int maxg = 0;                      // max over slots of g
   DArr<int> dcoarsest;               // per slot: index of its coarsest level
   DArr<int> dgstart;                 // per slot: g
+  DArr<int> dcta_order;              // slots in the CTA order of the coarse V-cycle (largest first)
   DArr<double> cinv;                 // per slot: coarsest-level solution operator (64 x 64)
   std::vector<int> maxcol;           // per level: max colours over smoothing slots
   std::vector<std::vector<int>> smoff;  // [level][colour] offset into wsm[level]
