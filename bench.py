@@ -455,6 +455,57 @@ def plain_gpu_sample(budget_s: float):
     return {"cases_per_s": 1.0 / seconds_per_case, "s_per_iter": samples, "seconds_per_case": seconds_per_case}
 
 
+def plain_kernel_rooflines(peaks):
+    """The plain FP64 form's residual array and SOR sweep on the 1,029,000-cell tet channel's
+    momentum matrix (device pointers through the C-ABI), L2 flushed before every launch."""
+    import ctypes as ct
+    import torch
+    from matlab_ufvm_b200 import case, ufvm
+    spec = case.channel_case()
+    g = ufvm.GpuCase(spec)
+    g.iterate()  # builds the level structure once
+    g.cfdUpdateFields()
+    g.cfdAssembleEquation("U", 1)
+    rp = torch.from_numpy(g.level_array(0, "rowptr")).cuda()
+    col = torch.from_numpy(g.level_array(0, "col")).cuda()
+    ac = torch.from_numpy(g.get("ac")).cuda()
+    anb = torch.from_numpy(g.get("anb")).cuda()
+    bc = torch.from_numpy(g.get("bc")).cuda()
+    g.close()
+    n, nnz = ac.numel(), anb.numel()
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    r = torch.empty_like(x)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    lib = ufvm.lib()
+    st = torch.cuda.current_stream()
+    P = lambda t: ct.c_void_p(t.data_ptr())
+    out = []
+    for name, call, by in (
+            ("k_residual (plain FP64 r = b - A x, cfdComputeResidualsArray)",
+             lambda: lib.ufvm_compute_residuals_array(n, P(rp), P(col), P(ac), P(anb), P(bc), P(x), P(r),
+                                                      ct.c_void_p(st.cuda_stream)),
+             36.0 * n + 12.0 * nnz),
+            ("k_sched_sweep<GS> (plain FP64 symmetric natural-order Gauss-Seidel, level scheduled, cfdSolveSOR)",
+             lambda: lib.ufvm_solve_sor(n, P(rp), P(col), P(ac), P(anb), P(bc), P(x), ct.c_void_p(st.cuda_stream)),
+             2.0 * (36.0 * n + 12.0 * nnz))):
+        assert call() == 0
+        times = []
+        for _ in range(5):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            assert call() == 0
+            e1.record(st)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        a = by / (ms * 1e-3) / 1e9
+        out.append({"kernel": name, "rows": n, "nnz": nnz, "bytes": by, "ms": round(ms, 4),
+                    "achieved": round(a, 1), "unit": "GB/s",
+                    "frac": round(a / peaks["hbm_gbs"], 4) if peaks.get("hbm_gbs") else None})
+    return out
+
+
 def pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
@@ -538,6 +589,7 @@ def main_ours(args):
     if rank == 0 and ws == 1:
         if not args.no_plain:
             plain = plain_gpu_sample(20.0)
+            plain["kernels"] = plain_kernel_rooflines(peaks)
         if not args.no_cpu:
             workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
             cpu = cpu_baseline(workers, 2.0)
@@ -568,7 +620,8 @@ def main_ours(args):
                 "value": plain["cases_per_s"], "unit": "cases/s",
                 "method": "plain FP64 form (reference SOR/ILU smoothers, AMG rebuilt every p solve) one case at a "
                           "time: seconds per SIMPLE iteration at n in 16..256 applied to the sweep's iteration counts",
-                "s_per_iter": {str(k): round(s, 6) for k, s in plain["s_per_iter"].items()}}
+                "s_per_iter": {str(k): round(s, 6) for k, s in plain["s_per_iter"].items()},
+                "kernels_1M_tet_channel": plain["kernels"]}
             line["batched_over_plain"] = value / plain["cases_per_s"] if plain["cases_per_s"] else None
         print(json.dumps(line), flush=True)
     if ws > 1:

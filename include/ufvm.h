@@ -230,10 +230,12 @@ int ufvm_service_poll(ufvm_service* s, int64_t* tickets, int64_t capacity, int64
 int ufvm_service_set_admit_interval(ufvm_service* s, int32_t steps);
 /* Launch schedule of the p solve's V-cycle: AMG levels of at most cta_rows rows are smoothed
  * by one thread block per case (all of a case's small levels in one launch), larger levels by
- * grid-wide launches over all cases. By default an autotuner picks cta_rows by timing the
- * candidates 2048 .. 65536 on the live batch (re-tuned every 2000 steps); a positive value
+ * grid-wide launches over all cases. packed 1 (default) packs up to four small cases into one
+ * 1024-thread block (256 threads and a named barrier each) and gives a large case a whole
+ * block; 0 runs one block per case. By default an autotuner picks cta_rows by timing the
+ * candidates 2048 .. 65536 on the live batch (re-tuned every 2000 steps); a positive cta_rows
  * fixes the schedule, 0 hands it back to the autotuner. The schedule changes no result. */
-int ufvm_service_set_schedule(ufvm_service* s, int32_t cta_rows);
+int ufvm_service_set_schedule(ufvm_service* s, int32_t cta_rows, int32_t packed);
 /* The CUDA stream (cudaStream_t) on which the service issues all of its device work, so a
  * caller can order its own work or timing events after a step. No counterpart in the
  * reference (its solves are synchronous MATLAB calls). */

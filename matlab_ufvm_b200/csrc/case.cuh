@@ -129,6 +129,9 @@ struct BatchLaunch {
   int nslots;
   double* part;              // block partials, >= 2 * max(nwc, nwu) entries
   cudaStream_t st;
+  // optional (host): vel_mask[3 * ip + mode - 1] != 0 when some slot's patch ip has work in
+  // boundary-velocity correction mode `mode`; launches without work are skipped
+  const unsigned char* vel_mask = nullptr;
 };
 
 struct Case {

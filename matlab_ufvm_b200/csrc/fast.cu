@@ -416,7 +416,9 @@ __device__ __forceinline__ int color_row(const LevDesc& A, int c, int t) {
 }
 
 // one Gauss-Seidel update of row (storage index) p
-__device__ __forceinline__ void gs_row32(const LevDesc& A, int p) { A.x[p] = row_sum32(A, p, A.bc[p]) / A.ac[p]; }
+__device__ __forceinline__ void gs_row32(const LevDesc& A, int p) {
+  A.x[p] = row_sum32(A, p, A.bc[p]) / A.ac[p];
+}
 
 __device__ __forceinline__ void res_row32(const LevDesc& A, int p) {
   A.r[p] = row_sum32(A, p, A.bc[p] - A.ac[p] * A.x[p]);
@@ -438,56 +440,16 @@ __device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C
   F.x[p] = F.x[p] + C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
 }
 
-// Two ELL rows at once: all column and coefficient loads of both rows are issued before the
-// neighbour gathers of either, doubling the loads each thread keeps in flight.
-__device__ __forceinline__ void row_sum32_x2(const LevDesc& A, int p0, float& v0, int p1, float& v1, bool two) {
-  const int W = A.ellW;
-  const size_t n = (size_t)A.n;
-  int c0[kEllUnroll], c1[kEllUnroll];
-  float a0[kEllUnroll], a1[kEllUnroll];
-#pragma unroll
-  for (int k = 0; k < kEllUnroll; ++k) {
-    c0[k] = k < W ? A.ellCol[k * n + p0] : -1;
-    a0[k] = k < W ? A.ellAnb[k * n + p0] : 0.0f;
-    c1[k] = (two && k < W) ? A.ellCol[k * n + p1] : -1;
-    a1[k] = (two && k < W) ? A.ellAnb[k * n + p1] : 0.0f;
-  }
-  float x0[kEllUnroll], x1[kEllUnroll];
-#pragma unroll
-  for (int k = 0; k < kEllUnroll; ++k) {
-    x0[k] = c0[k] >= 0 ? A.x[c0[k]] : 0.0f;
-    x1[k] = c1[k] >= 0 ? A.x[c1[k]] : 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < kEllUnroll; ++k) {
-    if (c0[k] >= 0) v0 = v0 - a0[k] * x0[k];
-    if (c1[k] >= 0) v1 = v1 - a1[k] * x1[k];
-  }
-}
-
-// One colour of a Gauss-Seidel sweep. Launched with kBlock / 2 threads per (slot, block) work
-// item of kBlock rows: each thread updates rows t and t + kBlock / 2 of the item.
-__global__ void __launch_bounds__(kBlock / 2) k_mc32(const LevDesc* __restrict__ levTab, int ns, int l,
-                                                     const int2* __restrict__ work, int color,
-                                                     const SolveCtl* __restrict__ ctl) {
+// One colour of a Gauss-Seidel sweep.
+__global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work, int color,
+                       const SolveCtl* __restrict__ ctl) {
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& A = LEV(l, w.x);
   if (color >= A.ncolor) return;
-  const int cnt = A.colorStart[color + 1] - A.colorStart[color];
-  const int t0 = w.y * kBlock + threadIdx.x, t1 = t0 + kBlock / 2;
-  if (t0 >= cnt) return;
-  const bool two = t1 < cnt;
-  if (A.pmode && A.ellW <= kEllUnroll) {
-    const int p0 = A.colorStart[color] + t0, p1 = A.colorStart[color] + t1;
-    float v0 = A.bc[p0], v1 = two ? A.bc[p1] : 0.0f;
-    row_sum32_x2(A, p0, v0, p1, v1, two);
-    A.x[p0] = v0 / A.ac[p0];
-    if (two) A.x[p1] = v1 / A.ac[p1];
-    return;
-  }
-  gs_row32(A, color_row(A, color, t0));
-  if (two) gs_row32(A, color_row(A, color, t1));
+  const int t = w.y * blockDim.x + threadIdx.x;
+  if (t >= A.colorStart[color + 1] - A.colorStart[color]) return;
+  gs_row32(A, color_row(A, color, t));
 }
 
 __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
@@ -611,10 +573,23 @@ __global__ void __launch_bounds__(1024) k_coarse_factor(const LevDesc* __restric
   for (int t = threadIdx.x; t < n * n; t += blockDim.x) out[t] = sm.X[t / n][t % n];
 }
 
-__device__ void coarse_apply_cta(const LevDesc& A, const double* __restrict__ X) {
+// Synchronisation domains of the coarse V-cycle: one CTA, or one thread group of a CTA with
+// its own named barrier. tid / nth: this thread's index and the domain's thread count.
+struct CtaDomain {
+  int tid, nth;
+  __device__ void sync() const { __syncthreads(); }
+};
+// a 256-thread group of a CTA with its own named barrier (ids 1..4; 0 is __syncthreads)
+struct GroupDomain {
+  int tid, nth, bar;
+  __device__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nth) : "memory"); }
+};
+
+template <class D>
+__device__ void coarse_apply(const LevDesc& A, const double* __restrict__ X, const D& d) {
   const int n = A.n;
   if (n > kDense) {
-    if (threadIdx.x == 0) {
+    if (d.tid == 0) {
       for (int sweep = 0; sweep < 40; ++sweep)
         for (int pass = 0; pass < 2; ++pass)
           for (int q = 0; q < n; ++q) {
@@ -624,34 +599,58 @@ __device__ void coarse_apply_cta(const LevDesc& A, const double* __restrict__ X)
             A.x[i] = (float)(v / A.ac64[i]);
           }
     }
-    __syncthreads();
+    d.sync();
     return;
   }
   // b is read in full before any x is written (A.bc and A.x are distinct arrays)
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = d.tid; i < n; i += d.nth) {
     double v = 0.0;
     for (int j = 0; j < n; ++j) v += X[(size_t)i * n + j] * (double)A.bc[j];
     A.x[i] = (float)v;
   }
-  __syncthreads();
+  d.sync();
 }
 
-__device__ void smooth_cta(const LevDesc& A, int sweeps) {
+template <class D>
+__device__ void smooth_dom(const LevDesc& A, int sweeps, const D& d) {
   for (int sw = 0; sw < sweeps; ++sw)
     for (int pass = 0; pass < 2; ++pass)
       for (int q = 0; q < A.ncolor; ++q) {
         const int c = pass == 0 ? q : A.ncolor - 1 - q;
         const int cnt = A.colorStart[c + 1] - A.colorStart[c];
-        for (int t = threadIdx.x; t < cnt; t += blockDim.x) gs_row32(A, color_row(A, c, t));
-        __syncthreads();
+        for (int t = d.tid; t < cnt; t += d.nth) gs_row32(A, color_row(A, c, t));
+        d.sync();
       }
 }
 
-// The small-level part of the V-cycle, one CTA per slot: levels g .. coarsest, where g is the
-// first level of the slot small enough for one CTA (levels above g run as grid-wide launches).
-// Descend with pre-smoothing, residual and restriction; apply the coarsest operator; ascend
-// with prolongation and post-smoothing. A slot whose coarsest level is 0 gets its direct solve
-// on level 0 here.
+// Levels g .. coarsest of slot s: descend with pre-smoothing, residual and restriction; apply
+// the coarsest operator; ascend with prolongation and post-smoothing. Every thread of the
+// domain takes the same path (the loops depend on the slot only), so the barriers match.
+template <class D>
+__device__ void vcycle_levels(const LevDesc* __restrict__ levTab, int ns, int s, int L, int g,
+                              const double* __restrict__ cinv, int pre, int post, const D& d) {
+  for (int l = g; l < L; ++l) {
+    const LevDesc& A = LEV(l, s);
+    const LevDesc& C = LEV(l + 1, s);
+    smooth_dom(A, pre, d);
+    for (int p = d.tid; p < A.n; p += d.nth) res_row32(A, p);
+    d.sync();
+    for (int P = d.tid; P < C.n; P += d.nth) restrict_row32(A, C, P);
+    d.sync();
+  }
+  coarse_apply(LEV(L, s), cinv + (size_t)s * kDense * kDense, d);
+  for (int l = L - 1; l >= g; --l) {
+    const LevDesc& A = LEV(l, s);
+    const LevDesc& C = LEV(l + 1, s);
+    for (int p = d.tid; p < A.n; p += d.nth) prolong_row32(A, C, p);
+    d.sync();
+    smooth_dom(A, post, d);
+  }
+}
+
+// The small-level part of the V-cycle, one CTA per slot (levels g .. coarsest, where g is the
+// first level of the slot small enough for this kernel; larger levels run as grid-wide
+// launches). A slot whose coarsest level is 0 gets its direct solve on level 0 here.
 __global__ void __launch_bounds__(1024, 2) k_coarse_vcycle(const LevDesc* __restrict__ levTab, int ns,
                                                         const int* __restrict__ coarsest,
                                                         const int* __restrict__ gstart, const double* __restrict__ cinv,
@@ -659,24 +658,27 @@ __global__ void __launch_bounds__(1024, 2) k_coarse_vcycle(const LevDesc* __rest
                                                         const int* __restrict__ order) {
   const int s = order[blockIdx.x];
   if (!ctl[s].active) return;
-  const int L = coarsest[s], g = gstart[s];
-  for (int l = g; l < L; ++l) {
-    const LevDesc& A = LEV(l, s);
-    const LevDesc& C = LEV(l + 1, s);
-    smooth_cta(A, pre);
-    for (int p = threadIdx.x; p < A.n; p += blockDim.x) res_row32(A, p);
-    __syncthreads();
-    for (int P = threadIdx.x; P < C.n; P += blockDim.x) restrict_row32(A, C, P);
-    __syncthreads();
-  }
-  coarse_apply_cta(LEV(L, s), cinv + (size_t)s * kDense * kDense);
-  for (int l = L - 1; l >= g; --l) {
-    const LevDesc& A = LEV(l, s);
-    const LevDesc& C = LEV(l + 1, s);
-    for (int p = threadIdx.x; p < A.n; p += blockDim.x) prolong_row32(A, C, p);
-    __syncthreads();
-    smooth_cta(A, post);
-  }
+  vcycle_levels(levTab, ns, s, coarsest[s], gstart[s], cinv, pre, post,
+                       CtaDomain{(int)threadIdx.x, (int)blockDim.x});
+}
+
+// The same with packed CTAs: a task either gives one large slot the whole CTA, or gives each of
+// its kPackGroups groups of kBlockPack / kPackGroups threads its own small slot (each group
+// synchronises on its own named barrier), so that many small cases share one CTA.
+__global__ void __launch_bounds__(kBlockPack, 1) k_coarse_vcycle_pk(const LevDesc* __restrict__ levTab, int ns,
+                                                                   const int* __restrict__ coarsest,
+                                                                   const int* __restrict__ gstart,
+                                                                   const double* __restrict__ cinv, int pre, int post,
+                                                                   const SolveCtl* __restrict__ ctl,
+                                                                   const PackTask* __restrict__ tasks) {
+  const PackTask& T = tasks[blockIdx.x];
+  // one code path for both: a large slot is one group of the whole CTA on barrier 1
+  const int gsize = T.big ? kBlockPack : kBlockPack / kPackGroups;
+  const int grp = threadIdx.x / gsize;
+  const int s = T.slot[grp];
+  if (s < 0 || !ctl[s].active) return;  // the same decision in every thread of the group
+  vcycle_levels(levTab, ns, s, coarsest[s], gstart[s], cinv, pre, post,
+                       GroupDomain{(int)threadIdx.x % gsize, gsize, 1 + grp});
 }
 
 // ---------------------------------------------------------------- host side
@@ -803,6 +805,31 @@ int Service::rebuild_tables() {
     for (int q = 0; q < ns; ++q) order[q] = q;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work_rows[a] > work_rows[b]; });
     UFVM_CHECK(upload_vec(dcta_order, order, stream));
+    // packed tasks: a slot with more than pk_rows rows below its grid levels gets a whole CTA,
+    // the others are packed kPackGroups to a CTA (largest first)
+    std::vector<PackTask> tasks;
+    PackTask cur{};
+    int fill = 0;
+    for (int q : order) {
+      if (work_rows[q] > pk_rows) {
+        PackTask t{};
+        t.big = 1;
+        for (int k = 0; k < kPackGroups; ++k) t.slot[k] = -1;
+        t.slot[0] = q;
+        tasks.push_back(t);
+        continue;
+      }
+      if (fill == 0) {
+        cur = PackTask{};
+        cur.big = 0;
+        for (int k = 0; k < kPackGroups; ++k) cur.slot[k] = -1;
+      }
+      cur.slot[fill++] = q;
+      if (fill == kPackGroups) { tasks.push_back(cur); fill = 0; }
+    }
+    if (fill) tasks.push_back(cur);
+    npk_tasks = (int)tasks.size();
+    UFVM_CHECK(upload_vec(dpk_tasks, tasks, stream));
   }
   UFVM_CHECK(dalloc(cinv, (size_t)ns * kDense * kDense));
   for (int l = 0; l < Lmax; ++l) {
@@ -851,6 +878,20 @@ int Service::rebuild_tables() {
     ucol_cnt[c] = (int)uc.size() - ucol_off[c];
   }
   UFVM_CHECK(upload_work(wu_col, uc, stream));
+  // boundary-velocity correction modes with work (k_vel_patch): 1 symmetry / empty / slip
+  // wall, 2 and 3 an outlet with fixed p
+  {
+    int maxp = 0;
+    for (auto* c : cases) maxp = std::max(maxp, c->P.n);
+    vel_mask.assign(3 * (size_t)maxp, 0);
+    for (auto* c : cases)
+      for (int ip = 0; ip < c->P.n; ++ip) {
+        const int ty = c->P.type[ip], tp = c->P.bcP[ip];
+        if (ty == UFVM_PATCH_SYMMETRY || ty == UFVM_PATCH_EMPTY || (ty == UFVM_PATCH_WALL && tp == UFVM_BC_SLIP))
+          vel_mask[3 * ip + 0] = 1;
+        if (ty == UFVM_PATCH_OUTLET && tp == UFVM_BC_FIXED_VALUE) vel_mask[3 * ip + 1] = vel_mask[3 * ip + 2] = 1;
+      }
+  }
   tables_dirty = false;
   graph_valid = false;
   UFVM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -859,8 +900,10 @@ int Service::rebuild_tables() {
 }
 
 BatchLaunch Service::batch() {
-  return BatchLaunch{slotTab.p, wc.p, nwc, wf.p, nwf, wb.p, nwb, wu.p, nwu, cstart.p, cend.p, ustart.p, uend.p,
-                     (int)cases.size(), part.p, stream};
+  BatchLaunch b{slotTab.p, wc.p, nwc, wf.p, nwf, wb.p, nwb, wu.p, nwu, cstart.p, cend.p, ustart.p, uend.p,
+                (int)cases.size(), part.p, stream};
+  b.vel_mask = vel_mask.empty() ? nullptr : vel_mask.data();
+  return b;
 }
 
 // The reference's agglomeration of the assembled p matrix, FP32 arrays and colourings.
@@ -1077,7 +1120,7 @@ int Service::solve_p(bool g) {
         for (int q = 0; q < maxcol[l]; ++q) {
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
-          k_mc32<<<smcnt[l][c], kBlock / 2, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+          k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
         }
   };
   // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
@@ -1094,8 +1137,13 @@ int Service::solve_p(bool g) {
       k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
       k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
     }
-    k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
-                                             s.p_post_sweep, pctl.p, dcta_order.p);
+    if (use_packing && npk_tasks > 0) {
+      k_coarse_vcycle_pk<<<npk_tasks, kBlockPack, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p,
+                                                              s.p_pre_sweep, s.p_post_sweep, pctl.p, dpk_tasks.p);
+    } else {
+      k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
+                                               s.p_post_sweep, pctl.p, dcta_order.p);
+    }
     for (int l = maxg - 1; l >= 0; --l) {
       k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
       smooth(l, s.p_post_sweep);
@@ -1410,7 +1458,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
         for (int q = 0; q < maxcol[0]; ++q) {
           const int c = pass == 0 ? q : maxcol[0] - 1 - q;
           if (smcnt[0][c] == 0) continue;
-          k_mc32<<<smcnt[0][c], kBlock / 2, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
+          k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
         }
     } else {
       k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,
@@ -1477,7 +1525,7 @@ Service::~Service() {
   for (auto& a : wsm) dfree(a);
   for (auto& a : wnc) dfree(a);
   for (auto& a : wrc) dfree(a);
-  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order);
+  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order); dfree(dpk_tasks);
   lin.release();
   for (auto e : evpool) destroy_check(cudaEventDestroy(e), "cudaEventDestroy");
   if (bstream) destroy_check(cudaStreamDestroy(bstream), "cudaStreamDestroy");

@@ -25,6 +25,15 @@ struct LevDesc {
   double *uAnb, *uAc, *uBc, *uX;  // level 0, pmode: FP64 ELL copy of the momentum matrix
 };
 
+// Packed coarse V-cycle: CTAs of kBlockPack threads; a task gives one large case the whole
+// CTA or each of kPackGroups thread groups its own small case (slot -1: none).
+constexpr int kBlockPack = 1024;
+constexpr int kPackGroups = 4;
+struct PackTask {
+  int big;
+  int slot[kPackGroups];
+};
+
 // Per-slot control state of the batched linear solves (device resident).
 struct SolveCtl {
   double r0, r1;
@@ -63,6 +72,9 @@ struct Service {
   DArr<int> dcoarsest;               // per slot: index of its coarsest level
   DArr<int> dgstart;                 // per slot: g
   DArr<int> dcta_order;              // slots in the CTA order of the coarse V-cycle (largest first)
+  DArr<PackTask> dpk_tasks;          // packed tasks of the coarse V-cycle
+  std::vector<unsigned char> vel_mask;  // boundary-velocity correction launches with work
+  int npk_tasks = 0;
   DArr<double> cinv;                 // per slot: coarsest-level solution operator (64 x 64)
   std::vector<int> maxcol;           // per level: max colours over smoothing slots
   std::vector<std::vector<int>> smoff;  // [level][colour] offset into wsm[level]
@@ -96,6 +108,10 @@ struct Service {
   // schedule: levels of at most cta_rows rows are smoothed inside the per-case CTA of the coarse
   // V-cycle kernel, larger ones by grid-wide launches over all cases
   int cta_rows = 8192;
+  // the coarse V-cycle packs small cases kPackGroups to a CTA (1) or runs one CTA per case (0);
+  // a case with more than pk_rows rows below its grid levels gets a whole CTA
+  int use_packing = 1;
+  int pk_rows = 1024;
   long long n_tunes = 0;
 
   int rebuild_tables();

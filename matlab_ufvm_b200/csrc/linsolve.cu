@@ -96,28 +96,61 @@ int scan_exclusive(LinCtx& c, const int* in, int* out, int n, int* total_host) {
 }
 
 // ---------------------------------------------------------------- residual
-__device__ __forceinline__ double row_residual(int i, const int* __restrict__ rp, const int* __restrict__ col,
-                                               const double* __restrict__ ac, const double* __restrict__ anb,
-                                               const double* __restrict__ bc, const double* __restrict__ x) {
+// The block's rows own one contiguous range of the CSR arrays. It is staged through shared
+// memory with unit-stride loads by the whole block (kStageEntries entries at most; a longer
+// range is read directly), then each thread sums its own row from shared memory in the
+// cconn order, so the result is the same bit for bit as the direct per-row loop.
+constexpr int kStageEntries = 8 * kBlock;
+
+__device__ __forceinline__ double block_row_residual(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                                                     const double* __restrict__ ac, const double* __restrict__ anb,
+                                                     const double* __restrict__ bc, const double* __restrict__ x,
+                                                     double* s_anb, int* s_col, bool* valid) {
+  const int r0 = blockIdx.x * blockDim.x;
+  const int r1 = min(n, r0 + (int)blockDim.x);
+  const int k0 = rp[r0], k1 = rp[r1];
+  const bool staged = k1 - k0 <= kStageEntries;  // uniform across the block
+  if (staged) {
+    for (int k = k0 + (int)threadIdx.x; k < k1; k += blockDim.x) {
+      s_anb[k - k0] = anb[k];
+      s_col[k - k0] = col[k];
+    }
+  }
+  __syncthreads();
+  const int i = r0 + threadIdx.x;
+  *valid = i < n;
+  if (i >= n) return 0.0;
   double v = bc[i] - ac[i] * x[i];
-  for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - anb[k] * x[col[k]];
+  if (staged) {
+    for (int k = rp[i] - k0; k < rp[i + 1] - k0; ++k) v = v - s_anb[k] * x[s_col[k]];
+  } else {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - anb[k] * x[col[k]];
+  }
   return v;
 }
 
-__global__ void k_residual(int n, const int* __restrict__ rp, const int* __restrict__ col,
-                           const double* __restrict__ ac, const double* __restrict__ anb,
-                           const double* __restrict__ bc, const double* __restrict__ x, double* __restrict__ r) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) r[i] = row_residual(i, rp, col, ac, anb, bc, x);
+__global__ void __launch_bounds__(kBlock) k_residual(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                                                     const double* __restrict__ ac, const double* __restrict__ anb,
+                                                     const double* __restrict__ bc, const double* __restrict__ x,
+                                                     double* __restrict__ r) {
+  __shared__ double s_anb[kStageEntries];
+  __shared__ int s_col[kStageEntries];
+  bool valid;
+  const double v = block_row_residual(n, rp, col, ac, anb, bc, x, s_anb, s_col, &valid);
+  if (valid) r[blockIdx.x * blockDim.x + threadIdx.x] = v;
 }
 
 // sum_i |r_i| : block partials (stage 1)
-__global__ void k_sumabs_res(int n, const int* __restrict__ rp, const int* __restrict__ col,
-                             const double* __restrict__ ac, const double* __restrict__ anb,
-                             const double* __restrict__ bc, const double* __restrict__ x, double* part) {
+__global__ void __launch_bounds__(kBlock) k_sumabs_res(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                                                       const double* __restrict__ ac, const double* __restrict__ anb,
+                                                       const double* __restrict__ bc, const double* __restrict__ x,
+                                                       double* part) {
+  __shared__ double s_anb[kStageEntries];
+  __shared__ int s_col[kStageEntries];
   __shared__ double sh[32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double v = i < n ? fabs(row_residual(i, rp, col, ac, anb, bc, x)) : 0.0;
+  bool valid;
+  const double r = block_row_residual(n, rp, col, ac, anb, bc, x, s_anb, s_col, &valid);
+  double v = valid ? fabs(r) : 0.0;
   v = block_reduce<0>(v, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }

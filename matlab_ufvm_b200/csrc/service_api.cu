@@ -374,8 +374,12 @@ int ufvm_service_set_admit_interval(ufvm_service* h, int32_t steps) {
   return UFVM_OK;
 }
 
-int ufvm_service_set_schedule(ufvm_service* h, int32_t cta_rows) {
-  if (!h || cta_rows < 0) return UFVM_E_INVALID;
+int ufvm_service_set_schedule(ufvm_service* h, int32_t cta_rows, int32_t packed) {
+  if (!h || cta_rows < 0 || packed < 0 || packed > 1) return UFVM_E_INVALID;
+  if (h->impl.svc.use_packing != packed) {
+    h->impl.svc.use_packing = packed;
+    h->impl.svc.tables_dirty = true;
+  }
   if (cta_rows == 0) {  // hand the schedule back to the autotuner
     h->impl.tune_on = true;
     h->impl.next_tune = h->impl.steps;

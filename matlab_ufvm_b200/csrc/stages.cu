@@ -736,11 +736,10 @@ int stage_correct_p(const BatchLaunch& b, int max_patches, double*) {
   UFVM_LAUNCH_CHECK();
   UFVM_CHECK(gradient<G_PP>(b));
   k_vel_cells<<<b.nwc, kBlock, 0, b.st>>>(b.slots, b.wc);
-  for (int ip = 0; ip < max_patches; ++ip) {
-    k_vel_patch<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, ip, 2);
-    k_vel_patch<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, ip, 3);
-    k_vel_patch<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, ip, 1);
-  }
+  for (int ip = 0; ip < max_patches; ++ip)
+    for (int mode : {2, 3, 1})
+      if (!b.vel_mask || b.vel_mask[3 * ip + mode - 1])
+        k_vel_patch<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, ip, mode);
   UFVM_LAUNCH_CHECK();
   k_p_cells<<<b.nwc, kBlock, 0, b.st>>>(b.slots, b.wc);
   k_p_bc<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb);

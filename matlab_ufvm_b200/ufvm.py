@@ -379,7 +379,7 @@ def _service_lib():
         L.ufvm_service_profile.argtypes = [VP, ct.c_int32, ct.c_int32, D, D]
         L.ufvm_service_poll.argtypes = [VP, ct.POINTER(ct.c_int64), ct.c_int64, ct.POINTER(ct.c_int64)]
         L.ufvm_service_set_admit_interval.argtypes = [VP, ct.c_int32]
-        L.ufvm_service_set_schedule.argtypes = [VP, ct.c_int32]
+        L.ufvm_service_set_schedule.argtypes = [VP, ct.c_int32, ct.c_int32]
         L._svc_ready = True
     return L
 
@@ -474,8 +474,9 @@ class Service:
         _check(_service_lib().ufvm_service_poll(self.h, buf, capacity, ct.byref(n)))
         return [int(buf[i]) for i in range(n.value)]
 
-    def set_schedule(self, cta_rows: int):
-        _check(_service_lib().ufvm_service_set_schedule(self.h, int(cta_rows)))
+    def set_schedule(self, cta_rows: int, packed: int = 1):
+        """Fix the V-cycle's launch schedule (cta_rows 0: back to the autotuner)."""
+        _check(_service_lib().ufvm_service_set_schedule(self.h, int(cta_rows), int(packed)))
 
     def set_admit_interval(self, steps: int):
         _check(_service_lib().ufvm_service_set_admit_interval(self.h, int(steps)))

@@ -80,3 +80,23 @@ def test_service_graph_ticks_match_eager_ticks(ufvm_mod):
             assert np.array_equal(x, y)
     for x, y in zip(rg, re_):
         assert np.array_equal(x, y)
+
+
+def test_service_schedules_give_same_bits(ufvm_mod):
+    """The V-cycle's launch schedule (grid launches vs one CTA per case vs thread-block
+    clusters) decides only where the work runs: every schedule gives the same bits."""
+    specs = [case.cavity_case(n, nu=1.0 / re, quirks=case.QUIRKS_CONVERGING)
+             for n, re in ((96, 300.0), (20, 100.0), (48, 700.0), (12, 60.0), (64, 900.0))]
+    out = []
+    for cta_rows, clusters in ((256, 0), (1 << 20, 0), (256, 1), (1 << 20, 1)):
+        svc = ufvm_mod.Service(ufvm_mod.fast_settings(specs[0]))
+        svc.set_schedule(cta_rows, clusters)
+        ts = [svc.submit(x, 3000) for x in specs]
+        for _ in range(12):
+            svc.step()
+        out.append([(svc.field(t, "U"), svc.field(t, "p"), svc.status(t)["res"]) for t in ts])
+        svc.close()
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y)
