@@ -105,6 +105,9 @@ typedef struct {
   double p_termination;        /* AMG termination (rrf) 0.1 */
   double u_rrf;                /* 0.1 */
   double false_dt;             /* 1e9 (cfdSetupTime.m:37) */
+  double p_coarse_weight;      /* service V-cycle: the prolongated coarse-grid correction is scaled
+                                  by this weight (over-correction of the piecewise-constant
+                                  prolongation); 0 or 1: unscaled, as cfdCorrectFinerLevelSolution.m */
 } ufvm_settings;
 
 typedef struct ufvm_case ufvm_case;

@@ -406,7 +406,7 @@ void free_level(Level& L, bool keep_matrix) {
   dfree(L.fwdStart); dfree(L.bwdRows); dfree(L.bwdStart); dfree(L.color); dfree(L.colorRows); dfree(L.colorStart);
   dfree(L.childStart); dfree(L.child); dfree(L.ac32); dfree(L.anb32); dfree(L.bc32); dfree(L.dphi32); dfree(L.r32);
   dfree(L.fr); dfree(L.fp); dfree(L.fq);
-  dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.childStartP);
+  dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.childStartP); dfree(L.gpos);
   dfree(L.ellAnb); dfree(L.uAnb); dfree(L.uAc); dfree(L.uBc); dfree(L.uX);
   L.ell_valid = false;
   L.sched_valid = false;

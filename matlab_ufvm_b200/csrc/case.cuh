@@ -56,7 +56,7 @@ struct Level {
   // childStartP / childP list each next-level storage index's children as positions
   bool ell_valid = false;
   int ellW = 0;
-  DArr<int> perm, inv, ellCol, parentsP, childP, childStartP;
+  DArr<int> perm, inv, ellCol, parentsP, childP, childStartP, gpos;
   DArr<float> ellAnb;
   DArr<double> uAnb, uAc, uBc, uX;  // level 0: FP64 ELL copy of the momentum matrix (service U solve)
 };

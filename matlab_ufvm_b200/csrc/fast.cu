@@ -337,14 +337,20 @@ __global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, 
     const int c = F.child[q];
     AC = AC + F.ac64[c];
     for (int k = F.rowptr[c]; k < F.rowptr[c + 1]; ++k) {
-      const int Q = F.parents[F.col[k]];
-      if (Q == P) {
-        AC = AC + F.anb64[k];
+      int pos;
+      if (F.gpos) {
+        pos = F.gpos[k];  // precomputed: -1 inside the aggregate, else the coarse entry
       } else {
-        int pos = c0;
-        while (pos < c1 && C.col[pos] != Q) ++pos;
-        if (pos < c1) C.anb64[pos] = C.anb64[pos] + F.anb64[k];
+        const int Q = F.parents[F.col[k]];
+        pos = -1;
+        if (Q != P) {
+          pos = c0;
+          while (pos < c1 && C.col[pos] != Q) ++pos;
+          if (pos == c1) pos = -2;
+        }
       }
+      if (pos == -1) AC = AC + F.anb64[k];
+      else if (pos >= 0) C.anb64[pos] = C.anb64[pos] + F.anb64[k];
     }
   }
   C.ac64[P] = AC;
@@ -437,7 +443,7 @@ __device__ __forceinline__ void restrict_row32(const LevDesc& F, const LevDesc& 
 }
 
 __device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C, int p) {
-  F.x[p] = F.x[p] + C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
+  F.x[p] = F.x[p] + F.pw * C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
 }
 
 // One colour of a Gauss-Seidel sweep.
@@ -767,12 +773,14 @@ int Service::rebuild_tables() {
         d.child = l + 1 < nl ? L.child.p : nullptr;
         d.colorRows = L.colorRows.p; d.colorStart = L.colorStart.p;
         if (l == 0) { d.fr = L.fr.p; d.fp = L.fp.p; d.fq = L.fq.p; }
+        d.pw = (S.p_coarse_weight > 0.0) ? (float)S.p_coarse_weight : 1.0f;
         d.pmode = (l + 1 < nl && L.ell_valid) ? 1 : 0;
         if (d.pmode) {
           d.ellW = L.ellW;
           d.perm = L.perm.p; d.inv = L.inv.p; d.ellCol = L.ellCol.p; d.ellAnb = L.ellAnb.p;
           d.parentsP = L.parentsP.p; d.childP = L.childP.p; d.childStartP = L.childStartP.p;
           if (l == 0) { d.uAnb = L.uAnb.p; d.uAc = L.uAc.p; d.uBc = L.uBc.p; d.uX = L.uX.p; }
+          d.gpos = L.gpos.p;
         }
       }
       lt[(size_t)l * ns + s] = d;
@@ -1032,6 +1040,24 @@ int Service::build_ell(Case& c) {
     UFVM_CHECK(upload_vec(L.parentsP, parP, stream));
     UFVM_CHECK(upload_vec(L.childP, chP, stream));
     UFVM_CHECK(upload_vec(L.childStartP, chS, stream));
+    {  // Galerkin target of every fine entry: -1 inside the aggregate, else the coarse position
+      std::vector<int> crp(nc + 1), ccol(std::max(C.nnz, 1));
+      UFVM_CUDA(cudaMemcpyAsync(crp.data(), C.rowptr.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      if (C.nnz)
+        UFVM_CUDA(cudaMemcpyAsync(ccol.data(), C.col.p, C.nnz * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      UFVM_CUDA(cudaStreamSynchronize(stream));
+      std::vector<int> gp(std::max(nnz, 1), -2);
+      for (int i = 0; i < n; ++i) {
+        const int Pi = parents[i];
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+          const int Q = parents[col[k]];
+          if (Q == Pi) { gp[k] = -1; continue; }
+          for (int t = crp[Pi]; t < crp[Pi + 1]; ++t)
+            if (ccol[t] == Q) { gp[k] = t; break; }
+        }
+      }
+      UFVM_CHECK(upload_vec(L.gpos, gp, stream));
+    }
     UFVM_CHECK(dalloc(L.ellAnb, std::max<size_t>((size_t)W * n, 1)));
     if (l == 0) {  // FP64 ELL copy of the momentum matrix for the U solve
       UFVM_CHECK(dalloc(L.uAnb, std::max<size_t>((size_t)W * n, 1)));

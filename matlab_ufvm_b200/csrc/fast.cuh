@@ -23,6 +23,8 @@ struct LevDesc {
   const int *perm, *inv, *ellCol, *parentsP, *childP, *childStartP;
   float* ellAnb;
   double *uAnb, *uAc, *uBc, *uX;  // level 0, pmode: FP64 ELL copy of the momentum matrix
+  const int* gpos;                // pmode: Galerkin target of each fine entry (-1: in the aggregate)
+  float pw;                       // weight of the prolongated coarse correction
 };
 
 // Packed coarse V-cycle: CTAs of kBlockPack threads; a task gives one large case the whole
