@@ -32,7 +32,7 @@ Case::~Case() {
   dfree(D.pnsum);
   for (int c = 0; c < 3; ++c) { dfree(U[c]); dfree(gp[c]); dfree(gPP[c]); dfree(DU[c]); dfree(vU[c]); }
   for (int k = 0; k < 9; ++k) dfree(gU[k]);
-  dfree(p); dfree(PP); dfree(mdot); dfree(fC1); dfree(fC2); dfree(vP); dfree(tmp3);
+  dfree(p); dfree(PP); dfree(mdot); dfree(fC1); dfree(fC2); dfree(vP); dfree(tmp3); dfree(uft);
   dfree(part); dfree(red); dfree(flags); dfree(scal); dfree(slot);
   dfree(wl.cells); dfree(wl.faces); dfree(wl.bfaces); dfree(wl.urows);
   dfree(wl.cstart); dfree(wl.cend); dfree(wl.ustart); dfree(wl.uend);

@@ -93,6 +93,7 @@ struct FieldView {
   double *DU0, *DU1, *DU2, *mdot, *fC1, *fC2;
   const double *vU0, *vU1, *vU2, *vP;  // boundary values (per boundary face)
   double* tmp3;                        // [Fb][3] staging for outlet velocity rows
+  double* uft;                         // [7][F] per-face momentum terms of one component
 };
 
 // Per-case descriptor read by the batched kernels. A stage kernel is launched over a
@@ -145,7 +146,7 @@ struct Case {
   std::vector<int> h_cfStart, h_cfFace, h_rowptr, h_col, h_ownSlot, h_neiSlot;
   // fields
   int rowsU = 0, rowsUcap = 0, q12_max_row = -1;
-  DArr<double> U[3], gU[9], p, gp[3], PP, gPP[3], DU[3], mdot, fC1, fC2, vU[3], vP, tmp3;
+  DArr<double> U[3], gU[9], p, gp[3], PP, gPP[3], DU[3], mdot, fC1, fC2, vU[3], vP, tmp3, uft;
   double scaleU = 1.0;
   // linear systems / hierarchy
   std::vector<Level> lev;

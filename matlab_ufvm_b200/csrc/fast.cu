@@ -254,6 +254,33 @@ __global__ void k_mc64(const SlotDesc* __restrict__ slots, const LevDesc* __rest
   S.dphi[i] = v / S.ac[i];
 }
 
+// One colour of the FP64 U Gauss-Seidel from self-contained work items (the ELL copy of the
+// momentum matrix; same row arithmetic as k_mc64).
+__global__ void k_mc64_items(const U0Item* __restrict__ items, const SolveCtl* __restrict__ ctl) {
+  const U0Item& it = items[blockIdx.x];
+  const int t = threadIdx.x;
+  if (t >= it.cnt || !ctl[it.slot].active) return;
+  const int p = it.p0 + t;
+  const size_t n = (size_t)it.n;
+  const int W = it.W;
+  int c[kEllUnroll];
+  double a[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) {
+    c[k] = k < W ? it.ellCol[k * n + p] : -1;
+    a[k] = k < W ? it.anb[k * n + p] : 0.0;
+  }
+  double v = it.bc[p];
+  const double d = it.ac[p];
+  double xv[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? it.x[c[k]] : 0.0;
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k)
+    if (c[k] >= 0) v = v - a[k] * xv[k];
+  it.x[p] = v / d;
+}
+
 // per-slot sums of block partials (fixed order)
 __global__ void k_slot_sum(const int* __restrict__ ws, const int* __restrict__ we, const double* __restrict__ part,
                            double* out) {
@@ -444,6 +471,34 @@ __device__ __forceinline__ void restrict_row32(const LevDesc& F, const LevDesc& 
 
 __device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C, int p) {
   F.x[p] = F.x[p] + F.pw * C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
+}
+
+// One colour of a level-0 Gauss-Seidel sweep from self-contained work items: the item carries
+// the row range and the level's array pointers, so the only loads before the row data are the
+// item and the case's active flag (issued together).
+__global__ void k_mc32_l0(const L0Item* __restrict__ items, const SolveCtl* __restrict__ ctl) {
+  const L0Item& it = items[blockIdx.x];
+  const int t = threadIdx.x;
+  if (t >= it.cnt || !ctl[it.slot].active) return;
+  const int p = it.p0 + t;
+  const size_t n = (size_t)it.n;
+  const int W = it.W;
+  int c[kEllUnroll];
+  float a[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) {
+    c[k] = k < W ? it.ellCol[k * n + p] : -1;
+    a[k] = k < W ? it.ellAnb[k * n + p] : 0.0f;
+  }
+  float v = it.bc[p];
+  const float d = it.ac[p];
+  float xv[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? it.x[c[k]] : 0.0f;
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k)
+    if (c[k] >= 0) v = v - a[k] * xv[k];
+  it.x[p] = v / d;
 }
 
 // One colour of a Gauss-Seidel sweep.
@@ -856,6 +911,7 @@ int Service::rebuild_tables() {
       if (l < hg[q] && cases[q]->lev[l].color_valid) mc = std::max(mc, cases[q]->lev[l].ncolor);
     maxcol[l] = mc;
     std::vector<int2> sm;
+    std::vector<L0Item> sm0;
     smoff[l].assign(mc, 0); smcnt[l].assign(mc, 0);
     for (int c = 0; c < mc; ++c) {
       smoff[l][c] = (int)sm.size();
@@ -863,29 +919,64 @@ int Service::rebuild_tables() {
         Level& L = cases[q]->lev[l];
         if (!(l < hg[q]) || !L.color_valid || c >= L.ncolor) continue;
         const int cnt = L.h_colorStart[c + 1] - L.h_colorStart[c];
-        for (int bb = 0; bb < nblocks(cnt); ++bb) sm.push_back(make_int2(q, bb));
+        for (int bb = 0; bb < nblocks(cnt); ++bb) {
+          sm.push_back(make_int2(q, bb));
+          if (l == 0 && L.ell_valid && L.ellW <= kEllUnroll) {  // self-contained level-0 item
+            L0Item it{};
+            it.slot = q;
+            it.p0 = L.h_colorStart[c] + bb * kBlock;
+            it.cnt = std::min(kBlock, cnt - bb * kBlock);
+            it.n = L.n;
+            it.W = L.ellW;
+            it.x = L.dphi32.p; it.bc = L.bc32.p; it.ac = L.ac32.p;
+            it.ellCol = L.ellCol.p; it.ellAnb = L.ellAnb.p;
+            sm0.push_back(it);
+          }
+        }
       }
       smcnt[l][c] = (int)sm.size() - smoff[l][c];
     }
     nwsm[l] = (int)sm.size();
     UFVM_CHECK(upload_work(wsm[l], sm, stream));
+    if (l == 0) {
+      // the self-contained items replace the (slot, block) list only when every item has one
+      l0_items = (int)sm0.size() == nwsm[0] && nwsm[0] > 0;
+      if (l0_items) UFVM_CHECK(upload_vec(wsm0, sm0, stream));
+    }
   }
   // level-0 colour rows of every slot (FP64 U smoother)
   ucolors = 0;
   for (auto* c : cases) ucolors = std::max(ucolors, c->lev[0].color_valid ? c->lev[0].ncolor : 0);
   std::vector<int2> uc;
+  std::vector<U0Item> uci;
   ucol_off.assign(ucolors, 0); ucol_cnt.assign(ucolors, 0);
   for (int c = 0; c < ucolors; ++c) {
     ucol_off[c] = (int)uc.size();
     for (int s = 0; s < ns; ++s) {
-      Level& L = cases[s]->lev[0];
+      Case& cs = *cases[s];
+      Level& L = cs.lev[0];
       if (!L.color_valid || c >= L.ncolor) continue;
       const int cnt = L.h_colorStart[c + 1] - L.h_colorStart[c];
-      for (int bb = 0; bb < nblocks(cnt); ++bb) uc.push_back(make_int2(s, bb));
+      const bool ell = cs.hierarchy_valid && cs.n_levels > 1 && L.ell_valid && L.ellW <= kEllUnroll;
+      for (int bb = 0; bb < nblocks(cnt); ++bb) {
+        uc.push_back(make_int2(s, bb));
+        if (ell) {
+          U0Item it{};
+          it.slot = s;
+          it.p0 = L.h_colorStart[c] + bb * kBlock;
+          it.cnt = std::min(kBlock, cnt - bb * kBlock);
+          it.n = L.n;
+          it.W = L.ellW;
+          it.x = L.uX.p; it.bc = L.uBc.p; it.ac = L.uAc.p; it.anb = L.uAnb.p; it.ellCol = L.ellCol.p;
+          uci.push_back(it);
+        }
+      }
     }
     ucol_cnt[c] = (int)uc.size() - ucol_off[c];
   }
   UFVM_CHECK(upload_work(wu_col, uc, stream));
+  u_items = (int)uci.size() == (int)uc.size() && !uc.empty();
+  if (u_items) UFVM_CHECK(upload_vec(wu_items, uci, stream));
   // boundary-velocity correction modes with work (k_vel_patch): 1 symmetry / empty / slip
   // wall, 2 and 3 an outlet with fixed p
   {
@@ -1091,7 +1182,8 @@ int Service::solve_u(bool g) {
       for (int q = 0; q < ucolors; ++q) {
         const int c = pass == 0 ? q : ucolors - 1 - q;
         if (ucol_cnt[c] == 0) continue;
-        k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
+        if (u_items) k_mc64_items<<<ucol_cnt[c], kBlock, 0, stream>>>(wu_items.p + ucol_off[c], uctl.p);
+        else k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
       }
     k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
     k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
@@ -1146,7 +1238,8 @@ int Service::solve_p(bool g) {
         for (int q = 0; q < maxcol[l]; ++q) {
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
-          k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+          if (l == 0 && l0_items) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(wsm0.p + smoff[0][c], pctl.p);
+          else k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
         }
   };
   // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
@@ -1477,14 +1570,17 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
         for (int q = 0; q < ucolors; ++q) {
           const int c = pass == 0 ? q : ucolors - 1 - q;
           if (ucol_cnt[c] == 0) continue;
-          k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
+          if (u_items) k_mc64_items<<<ucol_cnt[c], kBlock, 0, stream>>>(wu_items.p + ucol_off[c], uctl.p);
+          else
+            k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
         }
     } else if (kernel == 1) {
       for (int pass = 0; pass < 2; ++pass)
         for (int q = 0; q < maxcol[0]; ++q) {
           const int c = pass == 0 ? q : maxcol[0] - 1 - q;
           if (smcnt[0][c] == 0) continue;
-          k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
+          if (l0_items) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(wsm0.p + smoff[0][c], pctl.p);
+          else k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
         }
     } else {
       k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,
@@ -1551,7 +1647,7 @@ Service::~Service() {
   for (auto& a : wsm) dfree(a);
   for (auto& a : wnc) dfree(a);
   for (auto& a : wrc) dfree(a);
-  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order); dfree(dpk_tasks);
+  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order); dfree(dpk_tasks); dfree(wsm0); dfree(wu_items);
   lin.release();
   for (auto e : evpool) destroy_check(cudaEventDestroy(e), "cudaEventDestroy");
   if (bstream) destroy_check(cudaStreamDestroy(bstream), "cudaStreamDestroy");

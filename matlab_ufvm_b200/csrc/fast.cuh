@@ -36,6 +36,24 @@ struct PackTask {
   int slot[kPackGroups];
 };
 
+// A self-contained work item of the level-0 FP32 Gauss-Seidel (colour-permuted ELL): up to
+// kBlock rows p0 .. p0 + cnt - 1 of one case's level 0, with that level's arrays.
+struct L0Item {
+  int slot, p0, cnt, n, W, pad0;
+  float* x;
+  const float *bc, *ac;
+  const int* ellCol;
+  const float* ellAnb;
+};
+
+// The same for the FP64 U smoother on the ELL copy of the momentum matrix.
+struct U0Item {
+  int slot, p0, cnt, n, W, pad0;
+  double* x;
+  const double *bc, *ac, *anb;
+  const int* ellCol;
+};
+
 // Per-slot control state of the batched linear solves (device resident).
 struct SolveCtl {
   double r0, r1;
@@ -76,6 +94,10 @@ struct Service {
   DArr<int> dcta_order;              // slots in the CTA order of the coarse V-cycle (largest first)
   DArr<PackTask> dpk_tasks;          // packed tasks of the coarse V-cycle
   std::vector<unsigned char> vel_mask;  // boundary-velocity correction launches with work
+  DArr<L0Item> wsm0;                 // level-0 smoothing items (same order as wsm[0])
+  bool l0_items = false;
+  DArr<U0Item> wu_items;             // U smoothing items (same order as wu_col)
+  bool u_items = false;
   int npk_tasks = 0;
   DArr<double> cinv;                 // per slot: coarsest-level solution operator (64 x 64)
   std::vector<int> maxcol;           // per level: max colours over smoothing slots

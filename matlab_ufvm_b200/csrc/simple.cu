@@ -42,6 +42,7 @@ FieldView Case::fv() {
   v.mdot = mdot.p; v.fC1 = fC1.p; v.fC2 = fC2.p;
   v.vU0 = vU[0].p; v.vU1 = vU[1].p; v.vU2 = vU[2].p; v.vP = vP.p;
   v.tmp3 = tmp3.p;
+  v.uft = uft.p;
   return v;
 }
 
@@ -218,6 +219,7 @@ int Case::init_fields(const int32_t* bcu, const int32_t* bcp, const double* vu, 
     UFVM_CUDA(cudaMemsetAsync(DU[c].p, 0, R * sizeof(double), stream));
   }
   UFVM_CHECK(dalloc(mdot, F));
+  UFVM_CHECK(dalloc(uft, 7 * (size_t)F));
   UFVM_CHECK(dalloc(fC1, F));
   UFVM_CHECK(dalloc(fC2, F));
   UFVM_CUDA(cudaMemsetAsync(fC1.p, 0, F * sizeof(double), stream));

@@ -258,9 +258,121 @@ __device__ __forceinline__ void face_grad_corr(const MeshView& m, int fc, int o,
   r2 = (a2 - agm * e2) + lgm * e2;
 }
 
-// cfdAssembleEquation('U', comp): convection (upwind) + convection divergence, diffusion,
-// explicit stress, pressure gradient, false transient, URF, scaled residual, DU.
-__global__ void __launch_bounds__(kBlock, 3) k_assemble_u(const SlotDesc* __restrict__ slots,
+// The part of cfdAssembleEquation('U', comp) that depends on one face only: the upwind
+// convection coefficients and flux (cfdAssembleConvectionTerm.m:103-232), the diffusion
+// coefficients and flux (cfdAssembleDiffusionTerm.m:94-690; Q3, Q4, Q14, Q15) and the explicit
+// stress flux (cfdAssembleExplicitStressTerm.m:13-49, Q2), computed once per face (each
+// interior face serves two cells) into uft[k][F]:
+//   k = 0, 1, 2: convection C1, C2, T;  3, 4, 5: diffusion C1, C2, T;  6: stress T.
+// The cell kernel below adds them exactly as the reference's scatter does.
+enum { UF_C1 = 0, UF_C2 = 1, UF_T = 2, UF_D1 = 3, UF_D2 = 4, UF_TD = 5, UF_TS = 6, UF_N = 7 };
+
+__global__ void __launch_bounds__(kBlock, 3) k_uface(const SlotDesc* __restrict__ slots,
+                                                     const int2* __restrict__ work, int comp) {
+  SLOT_BEGIN(work);
+  const int fc = idx;
+  if (fc >= m.F) return;
+  const FieldView& f = S.f;
+  const int quirks = S.quirks;
+  const double* ph = Uc(f, comp);
+  const double nu = S.nu;
+  const double psi = f.mdot[fc];
+  const bool q4 = (quirks & UFVM_Q4_GRAD_WEIGHTS_SWAPPED) != 0;
+  const double* g0 = f.gU[comp * 3];
+  const double* g1 = f.gU[comp * 3 + 1];
+  const double* g2 = f.gU[comp * 3 + 2];
+  const bool q2 = (quirks & UFVM_Q2_STRESS_NOT_TRANSPOSED) != 0;
+  const double* s0 = q2 ? f.gU[comp * 3 + 0] : f.gU[0 * 3 + comp];
+  const double* s1 = q2 ? f.gU[comp * 3 + 1] : f.gU[1 * 3 + comp];
+  const double* s2 = q2 ? f.gU[comp * 3 + 2] : f.gU[2 * 3 + comp];
+  double* u = f.uft;
+  const size_t F = (size_t)m.F;
+  if (fc < m.Fi) {
+    const int o = m.owner[fc], n = m.neigh[fc];
+    {  // (1) convection, sign +1
+      const double C1 = 1.0 * dmax(psi, 0.0);
+      const double C2 = -1.0 * dmax(-psi, 0.0);
+      const double T = (C1 * ph[o] + C2 * ph[n]) + 0.0;
+      u[UF_C1 * F + fc] = C1; u[UF_C2 * F + fc] = C2; u[UF_T * F + fc] = T;
+    }
+    const double w = m.gf[fc];
+    const double gam = w * nu + (1 - w) * nu;
+    {  // (2) diffusion, sign -1
+      double gf0, gf1, gf2;
+      face_grad_corr(m, fc, o, n, g0, g1, g2, ph, q4, gf0, gf1, gf2);
+      const double C1 = (1.0 * gam) * m.gDiff[fc];
+      const double C2 = (-1.0 * gam) * m.gDiff[fc];
+      const double V = (-1.0 * gam) * dot3(gf0, gf1, gf2, m.Tx[fc], m.Ty[fc], m.Tz[fc]);
+      const double T = (C1 * ph[o] + C2 * ph[n]) + V;
+      u[UF_D1 * F + fc] = C1; u[UF_D2 * F + fc] = C2; u[UF_TD * F + fc] = T;
+    }
+    {  // (3) explicit stress, sign -1
+      const double x0 = w * s0[n] + (1 - w) * s0[o], x1 = w * s1[n] + (1 - w) * s1[o];
+      const double x2 = w * s2[n] + (1 - w) * s2[o];
+      u[UF_TS * F + fc] = (-1.0 * gam) * ((x0 * m.Sx[fc] + x1 * m.Sy[fc]) + x2 * m.Sz[fc]);
+    }
+    return;
+  }
+  const int e = m.owner[fc];
+  const int kb = fc - m.Fi, b = m.Nc + kb, p = m.bPatch[kb];
+  const int ty = m.ptype[p], tu = m.bcU[p];
+  {  // (1) convection
+    double C1 = 0.0, T = 0.0;
+    if (ty == UFVM_PATCH_INLET || ty == UFVM_PATCH_OUTLET) {
+      C1 = 1.0 * dmax(psi, 0.0);
+      const double C2 = -1.0 * dmax(-psi, 0.0);
+      T = (C1 * ph[e] + C2 * ph[b]) + 0.0;
+    }
+    u[UF_C1 * F + fc] = C1; u[UF_T * F + fc] = T;
+  }
+  const double gam = nu;
+  {  // (2) diffusion
+    double C1 = 0.0, T = 0.0;
+    if ((ty == UFVM_PATCH_WALL || ty == UFVM_PATCH_INLET) && tu == UFVM_BC_FIXED_VALUE) {
+      C1 = (1.0 * gam) * m.gDiff[fc];
+      const double C2 = (-1.0 * gam) * m.gDiff[fc];
+      const double V = (-1.0 * gam) * dot3(g0[b], g1[b], g2[b], m.Tx[fc], m.Ty[fc], m.Tz[fc]);
+      T = (C1 * ph[e] + C2 * ph[b]) + V;
+    } else if (ty == UFVM_PATCH_WALL && tu == UFVM_BC_NOSLIP) {
+      // cfdAssembleDiffusionTermWallNoslipBC (:479-562): Q3, Q14, Q15
+      const double A = m.area[fc];
+      const double n0 = m.Sx[fc] / A, n1 = m.Sy[fc] / A, n2 = m.Sz[fc] / A;
+      const int c2 = comp == 0 ? 1 : 0, c3 = comp == 2 ? 1 : 2;
+      const double nc = comp == 0 ? n0 : (comp == 1 ? n1 : n2);
+      const double nn2 = c2 == 0 ? n0 : n1;
+      const double nn3 = c3 == 1 ? n1 : n2;
+      const double dn = m.wd[fc];
+      const double TM = (quirks & UFVM_Q3_NOSLIP_GAMMA_TWICE) ? gam / dn : 1.0;
+      const double fac = (quirks & UFVM_Q14_NOSLIP_PATCH_SUM) ? (1 - m.pnsum[3 * p + comp]) : (1 - nc * nc);
+      const double third = (quirks & UFVM_Q15_NOSLIP_THIRD_SIGN) ? -1.0 : 1.0;
+      const double coef = ((1.0 * gam) * A / dn) * TM;
+      C1 = coef * fac;
+      const double* U2c = Uc(f, c2);
+      const double* U3c = Uc(f, c3);
+      const double inner = (ph[b] * fac + (U2c[e] - U2c[b]) * nn2 * nc) + third * ((U3c[e] - U3c[b]) * nn3 * nc);
+      const double bcf = coef * inner;
+      T = (C1 * ph[e] + 0.0 * ph[b]) + bcf;
+    } else if (ty == UFVM_PATCH_SYMMETRY || ty == UFVM_PATCH_EMPTY) {
+      const double A = m.area[fc];
+      const double n0 = m.Sx[fc] / A, n1 = m.Sy[fc] / A, n2 = m.Sz[fc] / A;
+      const double dd = dot3(m.CNx[fc], m.CNy[fc], m.CNz[fc], n0, n1, n2);
+      const double l0 = comp == 0 ? 0.0 : 1.0, l1 = comp == 1 ? 0.0 : 1.0, l2 = comp == 2 ? 0.0 : 1.0;
+      const double nc = comp == 0 ? n0 : (comp == 1 ? n1 : n2);
+      const double dv = dot3(f.U0[e] * l0, f.U1[e] * l1, f.U2[e] * l2, n0 * l0, n1 * l1, n2 * l2);
+      C1 = ((((1.0 * 2) * gam) * A) * (nc * nc)) / dd;
+      const double V = (((((-1.0 * 2) * gam) * A) * dv) * nc) / dd;
+      T = (C1 * ph[e] + 0.0 * ph[b]) + V;
+    }
+    u[UF_D1 * F + fc] = C1; u[UF_TD * F + fc] = T;
+  }
+  // (3) explicit stress
+  u[UF_TS * F + fc] = (-1.0 * gam) * ((s0[b] * m.Sx[fc] + s1[b] * m.Sy[fc]) + s2[b] * m.Sz[fc]);
+}
+
+// cfdAssembleEquation('U', comp): the face terms of k_uface scattered into the cell's row in
+// the reference's order -- convection over the cell's faces, the convection divergence,
+// diffusion, explicit stress -- then grad(p), false transient, URF, scaled residual, DU.
+__global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restrict__ slots,
                                                        const int2* __restrict__ work, int comp, double* part) {
   __shared__ double sh[32];
   SLOT_BEGIN(work);
@@ -268,32 +380,23 @@ __global__ void __launch_bounds__(kBlock, 3) k_assemble_u(const SlotDesc* __rest
   double rr = 0.0, rm = 0.0;
   if (e < m.Nc) {
     const FieldView& f = S.f;
-    const int quirks = S.quirks;
     const double* ph = Uc(f, comp);
     const int s = m.cfStart[e], ne = m.cfStart[e + 1];
     const int r0 = m.rowptr[e];
     double* anb = S.anb;
+    const double* u = f.uft;
+    const size_t F = (size_t)m.F;
     double acv = 0.0, bcv = 0.0, eff = 0.0;
-    // (1) convection, sign +1 (cfdAssembleConvectionTerm.m:103-232)
+    // (1) convection, sign +1
     for (int q = s; q < ne; ++q) {
       const int fc = m.cfFace[q];
       const double psi = f.mdot[fc];
+      const double C1 = u[UF_C1 * F + fc], T = u[UF_T * F + fc];
       if (fc < m.Fi) {
-        const int o = m.owner[fc], n = m.neigh[fc];
-        const double C1 = 1.0 * dmax(psi, 0.0);
-        const double C2 = -1.0 * dmax(-psi, 0.0);
-        const double T = (C1 * ph[o] + C2 * ph[n]) + 0.0;
-        if (o == e) { acv = acv + C1; anb[r0 + q - s] = 0.0 + C2; bcv = bcv - T; eff = eff + psi; }
+        const double C2 = u[UF_C2 * F + fc];
+        if (m.owner[fc] == e) { acv = acv + C1; anb[r0 + q - s] = 0.0 + C2; bcv = bcv - T; eff = eff + psi; }
         else { acv = acv - C2; anb[r0 + q - s] = 0.0 - C1; bcv = bcv + T; eff = eff - psi; }
       } else {
-        const int b = m.Nc + fc - m.Fi;
-        const int ty = m.ptype[m.bPatch[fc - m.Fi]];
-        double C1 = 0.0, T = 0.0;
-        if (ty == UFVM_PATCH_INLET || ty == UFVM_PATCH_OUTLET) {
-          C1 = 1.0 * dmax(psi, 0.0);
-          const double C2 = -1.0 * dmax(-psi, 0.0);
-          T = (C1 * ph[e] + C2 * ph[b]) + 0.0;
-        }
         acv = acv + C1;
         bcv = bcv - T;
         eff = eff + psi;
@@ -306,92 +409,29 @@ __global__ void __launch_bounds__(kBlock, 3) k_assemble_u(const SlotDesc* __rest
       acv = acv + fce;
       bcv = bcv - fte;
     }
-    // (2) diffusion, sign -1 (cfdAssembleDiffusionTerm.m:94-690)
-    const bool q4 = (quirks & UFVM_Q4_GRAD_WEIGHTS_SWAPPED) != 0;
-    const double* g0 = f.gU[comp * 3];
-    const double* g1 = f.gU[comp * 3 + 1];
-    const double* g2 = f.gU[comp * 3 + 2];
-    const double nu = S.nu;
+    // (2) diffusion, sign -1
     for (int q = s; q < ne; ++q) {
       const int fc = m.cfFace[q];
+      const double C1 = u[UF_D1 * F + fc], T = u[UF_TD * F + fc];
       if (fc < m.Fi) {
-        const int o = m.owner[fc], n = m.neigh[fc];
-        double gf0, gf1, gf2;
-        face_grad_corr(m, fc, o, n, g0, g1, g2, ph, q4, gf0, gf1, gf2);
-        const double w = m.gf[fc];
-        const double gam = w * nu + (1 - w) * nu;
-        const double C1 = (1.0 * gam) * m.gDiff[fc];
-        const double C2 = (-1.0 * gam) * m.gDiff[fc];
-        const double V = (-1.0 * gam) * dot3(gf0, gf1, gf2, m.Tx[fc], m.Ty[fc], m.Tz[fc]);
-        const double T = (C1 * ph[o] + C2 * ph[n]) + V;
+        const double C2 = u[UF_D2 * F + fc];
         const int k = r0 + q - s;
-        if (o == e) { acv = acv + C1; anb[k] = anb[k] + C2; bcv = bcv - T; }
+        if (m.owner[fc] == e) { acv = acv + C1; anb[k] = anb[k] + C2; bcv = bcv - T; }
         else { acv = acv - C2; anb[k] = anb[k] - C1; bcv = bcv + T; }
       } else {
-        const int kb = fc - m.Fi, b = m.Nc + kb, p = m.bPatch[kb];
-        const int ty = m.ptype[p], tu = m.bcU[p];
-        const double gam = nu;
-        double C1 = 0.0, T = 0.0;
-        if ((ty == UFVM_PATCH_WALL || ty == UFVM_PATCH_INLET) && tu == UFVM_BC_FIXED_VALUE) {
-          C1 = (1.0 * gam) * m.gDiff[fc];
-          const double C2 = (-1.0 * gam) * m.gDiff[fc];
-          const double V = (-1.0 * gam) * dot3(g0[b], g1[b], g2[b], m.Tx[fc], m.Ty[fc], m.Tz[fc]);
-          T = (C1 * ph[e] + C2 * ph[b]) + V;
-        } else if (ty == UFVM_PATCH_WALL && tu == UFVM_BC_NOSLIP) {
-          // cfdAssembleDiffusionTermWallNoslipBC (:479-562): Q3, Q14, Q15
-          const double A = m.area[fc];
-          const double n0 = m.Sx[fc] / A, n1 = m.Sy[fc] / A, n2 = m.Sz[fc] / A;
-          const int c2 = comp == 0 ? 1 : 0, c3 = comp == 2 ? 1 : 2;
-          const double nc = comp == 0 ? n0 : (comp == 1 ? n1 : n2);
-          const double nn2 = c2 == 0 ? n0 : n1;
-          const double nn3 = c3 == 1 ? n1 : n2;
-          const double dn = m.wd[fc];
-          const double TM = (quirks & UFVM_Q3_NOSLIP_GAMMA_TWICE) ? gam / dn : 1.0;
-          const double fac = (quirks & UFVM_Q14_NOSLIP_PATCH_SUM) ? (1 - m.pnsum[3 * p + comp]) : (1 - nc * nc);
-          const double third = (quirks & UFVM_Q15_NOSLIP_THIRD_SIGN) ? -1.0 : 1.0;
-          const double coef = ((1.0 * gam) * A / dn) * TM;
-          C1 = coef * fac;
-          const double* U2c = Uc(f, c2);
-          const double* U3c = Uc(f, c3);
-          const double inner = (ph[b] * fac + (U2c[e] - U2c[b]) * nn2 * nc) + third * ((U3c[e] - U3c[b]) * nn3 * nc);
-          const double bcf = coef * inner;
-          T = (C1 * ph[e] + 0.0 * ph[b]) + bcf;
-        } else if (ty == UFVM_PATCH_SYMMETRY || ty == UFVM_PATCH_EMPTY) {
-          const double A = m.area[fc];
-          const double n0 = m.Sx[fc] / A, n1 = m.Sy[fc] / A, n2 = m.Sz[fc] / A;
-          const double dd = dot3(m.CNx[fc], m.CNy[fc], m.CNz[fc], n0, n1, n2);
-          const double l0 = comp == 0 ? 0.0 : 1.0, l1 = comp == 1 ? 0.0 : 1.0, l2 = comp == 2 ? 0.0 : 1.0;
-          const double nc = comp == 0 ? n0 : (comp == 1 ? n1 : n2);
-          const double dv = dot3(f.U0[e] * l0, f.U1[e] * l1, f.U2[e] * l2, n0 * l0, n1 * l1, n2 * l2);
-          C1 = ((((1.0 * 2) * gam) * A) * (nc * nc)) / dd;
-          const double V = (((((-1.0 * 2) * gam) * A) * dv) * nc) / dd;
-          T = (C1 * ph[e] + 0.0 * ph[b]) + V;
-        }
         acv = acv + C1;
         bcv = bcv - T;
       }
     }
-    // (3) explicit stress div(nu*transp(grad(U))), sign -1 (cfdAssembleExplicitStressTerm.m:13-49, Q2)
-    const bool q2 = (quirks & UFVM_Q2_STRESS_NOT_TRANSPOSED) != 0;
-    const double* s0 = q2 ? f.gU[comp * 3 + 0] : f.gU[0 * 3 + comp];
-    const double* s1 = q2 ? f.gU[comp * 3 + 1] : f.gU[1 * 3 + comp];
-    const double* s2 = q2 ? f.gU[comp * 3 + 2] : f.gU[2 * 3 + comp];
+    // (3) explicit stress, sign -1
     for (int q = s; q < ne; ++q) {
       const int fc = m.cfFace[q];
+      const double T = u[UF_TS * F + fc];
       if (fc < m.Fi) {
-        const int o = m.owner[fc], n = m.neigh[fc];
-        const double w = m.gf[fc];
-        const double x0 = w * s0[n] + (1 - w) * s0[o], x1 = w * s1[n] + (1 - w) * s1[o];
-        const double x2 = w * s2[n] + (1 - w) * s2[o];
-        const double gam = w * nu + (1 - w) * nu;
-        const double T = (-1.0 * gam) * ((x0 * m.Sx[fc] + x1 * m.Sy[fc]) + x2 * m.Sz[fc]);
         const int k = r0 + q - s;
-        if (o == e) { acv = acv + 0.0; anb[k] = anb[k] + 0.0; bcv = bcv - T; }
+        if (m.owner[fc] == e) { acv = acv + 0.0; anb[k] = anb[k] + 0.0; bcv = bcv - T; }
         else { acv = acv - 0.0; anb[k] = anb[k] - 0.0; bcv = bcv + T; }
       } else {
-        const int b = m.Nc + fc - m.Fi;
-        const double gam = nu;
-        const double T = (-1.0 * gam) * ((s0[b] * m.Sx[fc] + s1[b] * m.Sy[fc]) + s2[b] * m.Sz[fc]);
         acv = acv + 0.0;
         bcv = bcv - T;
       }
@@ -708,6 +748,7 @@ int stage_update_fields(const BatchLaunch& b) {
 }
 
 int stage_assemble_u(const BatchLaunch& b, int comp) {
+  k_uface<<<b.nwf, kBlock, 0, b.st>>>(b.slots, b.wf, comp);
   k_assemble_u<<<b.nwc, kBlock, 0, b.st>>>(b.slots, b.wc, comp, b.part);
   k_du_boundary<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, comp);
   k_slot_final<0><<<b.nslots, 1024, 0, b.st>>>(b.slots, b.cstart, b.cend, b.part);
