@@ -97,13 +97,14 @@ def _mesh_worker(n):
     return n, case.cavity_case(n, nu=0.01, quirks=case.QUIRKS_CONVERGING)
 
 
-def prebuild_meshes(indices):
-    """Builds the cavity meshes the run needs, in a spawn pool (before any CUDA use)."""
+def prebuild_meshes(indices, ranks: int = 1):
+    """Builds the cavity meshes the run needs in a spawn pool, sharing the host cores with the
+    other ranks of the node."""
     import multiprocessing as mp
     need = sorted({stream_params(i)[0] for i in indices} - set(_SPEC_CACHE))
     if not need:
         return
-    procs = max(1, min(len(need), (os.cpu_count() or 2) - 1, 32))
+    procs = max(1, min(len(need), (os.cpu_count() or 2) // max(1, ranks) - 1, 32))
     if procs == 1 or len(need) < 4:
         for n in need:
             base_spec(n)
@@ -565,7 +566,7 @@ def main_ours(args):
     _b.build()
     # meshes for the first cases of this rank's share (the rest are built on demand)
     from matlab_ufvm_b200 import sharding
-    prebuild_meshes([sharding.stream_index(rank, ws, k) for k in range(1200)])
+    prebuild_meshes([sharding.stream_index(rank, ws, k) for k in range(1200 // ws + 1)], ws)
     peaks = load_peaks()
     svc, res = run_service(args, rank, ws, e2e=False)
     roof = roofline(svc, peaks) if rank == 0 else None

@@ -281,6 +281,37 @@ __global__ void k_mc64_items(const U0Item* __restrict__ items, const SolveCtl* _
   it.x[p] = v / d;
 }
 
+// sum |r| block partials of the U system from self-contained items (wc order; the same row
+// values and block sums as k_res64_abs on the ELL copy)
+__global__ void k_res64_items(const U0Item* __restrict__ items, const SolveCtl* __restrict__ ctl, double* part) {
+  __shared__ double sh[32];
+  const U0Item& it = items[blockIdx.x];
+  const int t = threadIdx.x;
+  double v = 0.0;
+  if (t < it.cnt && ctl[it.slot].active) {
+    const int p = it.p0 + t;
+    const size_t n = (size_t)it.n;
+    const int W = it.W;
+    int c[kEllUnroll];
+    double a[kEllUnroll];
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k) {
+      c[k] = k < W ? it.ellCol[k * n + p] : -1;
+      a[k] = k < W ? it.anb[k * n + p] : 0.0;
+    }
+    double r = it.bc[p] - it.ac[p] * it.x[p];
+    double xv[kEllUnroll];
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? it.x[c[k]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kEllUnroll; ++k)
+      if (c[k] >= 0) r = r - a[k] * xv[k];
+    v = fabs(r);
+  }
+  v = block_reduce<0>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
 // per-slot sums of block partials (fixed order)
 __global__ void k_slot_sum(const int* __restrict__ ws, const int* __restrict__ we, const double* __restrict__ part,
                            double* out) {
@@ -977,6 +1008,27 @@ int Service::rebuild_tables() {
   UFVM_CHECK(upload_work(wu_col, uc, stream));
   u_items = (int)uci.size() == (int)uc.size() && !uc.empty();
   if (u_items) UFVM_CHECK(upload_vec(wu_items, uci, stream));
+  {  // U residual items over every slot's rows, in the order of the wc list
+    std::vector<U0Item> ri;
+    bool all = true;
+    for (int s = 0; s < ns && all; ++s) {
+      Case& cs = *cases[s];
+      Level& L = cs.lev[0];
+      if (!(cs.hierarchy_valid && cs.n_levels > 1 && L.ell_valid && L.ellW <= kEllUnroll)) { all = false; break; }
+      for (int bb = 0; bb < nblocks(cs.M.Nc); ++bb) {
+        U0Item it{};
+        it.slot = s;
+        it.p0 = bb * kBlock;
+        it.cnt = std::min(kBlock, cs.M.Nc - bb * kBlock);
+        it.n = L.n;
+        it.W = L.ellW;
+        it.x = L.uX.p; it.bc = L.uBc.p; it.ac = L.uAc.p; it.anb = L.uAnb.p; it.ellCol = L.ellCol.p;
+        ri.push_back(it);
+      }
+    }
+    ures_items = all && (int)ri.size() == nwc;
+    if (ures_items) UFVM_CHECK(upload_vec(wures_items, ri, stream));
+  }
   // boundary-velocity correction modes with work (k_vel_patch): 1 symmetry / empty / slip
   // wall, 2 and 3 an outlet with fixed p
   {
@@ -1170,7 +1222,8 @@ int Service::solve_u(bool g) {
   k_u_to_ell<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p);
   // the first residual is taken for every slot
   k_set_active<<<nblocks(ns), kBlock, 0, stream>>>(uctl.p, ns);
-  k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
+  if (ures_items) k_res64_items<<<nwc, kBlock, 0, stream>>>(wures_items.p, uctl.p, part.p);
+  else k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
   k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
   // (in a captured tick the while node starts from its default condition 1: a body whose
   // slots are all inactive does nothing and its k_ctrl ends the loop)
@@ -1185,7 +1238,8 @@ int Service::solve_u(bool g) {
         if (u_items) k_mc64_items<<<ucol_cnt[c], kBlock, 0, stream>>>(wu_items.p + ucol_off[c], uctl.p);
         else k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
       }
-    k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
+    if (ures_items) k_res64_items<<<nwc, kBlock, 0, stream>>>(wures_items.p, uctl.p, part.p);
+    else k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
     k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
     k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 0, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
                                   SCAL_U_R1, anyflag.p, g, h, loopcnt.p, 0);
@@ -1647,7 +1701,7 @@ Service::~Service() {
   for (auto& a : wsm) dfree(a);
   for (auto& a : wnc) dfree(a);
   for (auto& a : wrc) dfree(a);
-  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order); dfree(dpk_tasks); dfree(wsm0); dfree(wu_items);
+  dfree(dcoarsest); dfree(dgstart); dfree(cinv); dfree(dcta_order); dfree(dpk_tasks); dfree(wsm0); dfree(wu_items); dfree(wures_items);
   lin.release();
   for (auto e : evpool) destroy_check(cudaEventDestroy(e), "cudaEventDestroy");
   if (bstream) destroy_check(cudaStreamDestroy(bstream), "cudaStreamDestroy");

@@ -98,6 +98,8 @@ struct Service {
   bool l0_items = false;
   DArr<U0Item> wu_items;             // U smoothing items (same order as wu_col)
   bool u_items = false;
+  DArr<U0Item> wures_items;          // U residual items (same order as wc)
+  bool ures_items = false;
   int npk_tasks = 0;
   DArr<double> cinv;                 // per slot: coarsest-level solution operator (64 x 64)
   std::vector<int> maxcol;           // per level: max colours over smoothing slots
