@@ -100,3 +100,27 @@ def test_service_schedules_give_same_bits(ufvm_mod):
         for a, b in zip(out[0], other):
             for x, y in zip(a, b):
                 assert np.array_equal(x, y)
+
+
+def test_service_mixed_meshes_same_alone_and_in_mix(ufvm_mod):
+    """2D and 3D cavities and a jittered-tet channel (inlet, fixed-p outlet, no-slip walls)
+    share the batch: after 30 steps every case holds the same bits as when it ran alone."""
+    specs = [case.channel_case(nx=10, ny=4, nz=4, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(24, nu=0.004, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(8, nu=0.005, dim=3, quirks=case.QUIRKS_CONVERGING)]
+
+    def run(batch):
+        svc = ufvm_mod.Service(ufvm_mod.fast_settings(batch[0]))
+        ts = [svc.submit(x, 3000) for x in batch]
+        for _ in range(30):
+            svc.step()
+        out = [(svc.field(t, "U"), svc.field(t, "p"), svc.field(t, "mdot")) for t in ts]
+        svc.close()
+        return out
+
+    alone = [run([x])[0] for x in specs]
+    mixed = run(specs)
+    for a, b in zip(alone, mixed):
+        for x, y in zip(a, b):
+            assert np.all(np.isfinite(x))
+            assert np.array_equal(x, y)
