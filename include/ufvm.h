@@ -201,9 +201,11 @@ int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col,
  * resident case advances one SIMPLE iteration per ufvm_service_step in one launch per stage,
  * and a case leaves the resident set when it converges (residualControl), fails, or reaches
  * its iteration limit, freeing room for queued cases. The solver settings are shared by all
- * cases of a service; nu and the boundary data are per case. Linear solves: multicolour
- * Gauss-Seidel (FP64) for U, FP32 AMG inside FP64 iterative refinement for p (the service
- * requires settings->precision == UFVM_PREC_FP32_AMG). Latencies are device time, summed
+ * cases of a service; nu, the boundary data and the pressure reference cell are per case (a
+ * case whose boundaries are all walls, empty or symmetry planes pins p at settings->
+ * fixed_element, or cell 0 if that is negative; any other case has none, cfdReadSystem.m:
+ * 238-252). Linear solves: multicolour Gauss-Seidel (FP64) for U, FP32 AMG preconditioning
+ * FP64 flexible CG for p (the service requires settings->precision == UFVM_PREC_FP32_AMG). Latencies are device time, summed
  * over the steps a case was resident; queue time is reported separately. */
 typedef struct ufvm_service ufvm_service;
 int ufvm_service_create(const ufvm_settings* settings, int64_t max_resident_cells, ufvm_service** out);

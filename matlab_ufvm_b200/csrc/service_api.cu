@@ -85,6 +85,13 @@ static int admit(ServiceImpl& S) {
     d.patch_n = p.pn.data();
     ufvm_settings cs = S.svc.S;
     cs.nu = p.nu;
+    // the pressure reference cell is per case, as in cfdReadSystem.m:238-252: a case whose
+    // boundaries are all walls, empty or symmetry planes pins p at the settings' pRefCell
+    // (cell 0 when the shared settings carry none); any other case has no reference cell
+    bool closed = true;
+    for (int32_t t : p.ptype)
+      if (t != UFVM_PATCH_WALL && t != UFVM_PATCH_EMPTY && t != UFVM_PATCH_SYMMETRY) closed = false;
+    cs.fixed_element = closed ? std::max(0, S.svc.S.fixed_element) : -1;
     Case* c = new Case();
     const int st = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr,
                                     nullptr, nullptr, S.svc.stream);

@@ -184,3 +184,96 @@ def write_polymesh(mesh: PolyMesh, case_dir: str) -> None:
             f.write(f"    {p.name}\n    {{\n        type            {p.type};\n"
                     f"        nFaces          {p.n};\n        startFace       {p.start};\n    }}\n")
         f.write(")\n")
+
+
+_BS = chr(92) * 2  # the reference's banner lines carry two backslashes
+_FOAM_BANNER = "\n".join([
+    "/*--------------------------------*- C++ -*----------------------------------*" + _BS,
+    "| =========                 |                                                 |",
+    "| " + _BS + "      /  F ield         | OpenFOAM: The Open Source CFD Toolbox           |",
+    "|  " + _BS + "    /   O peration     | Version:  v1706                                 |",
+    "|   " + _BS + "  /    A nd           | Web:      www.OpenFOAM.com                      |",
+    "|    " + _BS + "/     M anipulation  |                                                 |",
+    _BS + "*---------------------------------------------------------------------------*/",
+]) + "\n"
+
+_DIMENSIONS = {"U": "[0 1 -1 0 0 0 0]", "p": "[0 2 -2 0 0 0 0]", "mdot_f": "[1 0 -1 0 0 0 0]"}
+
+
+def _fmt(x: float, digits: int) -> str:
+    return f"{x:.{digits}g}"
+
+
+def _value_block(values: np.ndarray, ncomp: int, digits: int, indent: str) -> List[str]:
+    kind = "vector" if ncomp == 3 else "scalar"
+    out = [f"{indent}nonuniform List<{kind}>", str(len(values)), "("]
+    if ncomp == 3:
+        out += ["(" + " ".join(_fmt(v, digits) for v in row) + ")" for row in np.asarray(values).reshape(-1, 3)]
+    else:
+        out += [_fmt(v, digits) for v in np.asarray(values).ravel()]
+    return out + [")", ";"]
+
+
+def write_field(path: str, name: str, cls: str, internal: np.ndarray, boundary: List[Tuple[str, str, object]],
+                location: str = "0", dimensions: str = None, digits: int = 17) -> None:
+    """Write a field in the layout of postProcess/cfdWriteOpenFoamField.m (header, dimensions,
+    ``internalField nonuniform List<...>``, then per patch ``type`` and an optional nonuniform
+    ``value``). ``boundary`` lists (patch name, type, values or None) in patch order.
+    ``digits`` 17 writes every double exactly (a restart continues bit for bit); the reference
+    prints 5 significant digits (MATLAB num2str), which ``digits=5`` reproduces."""
+    ncomp = 3 if "Vector" in cls else 1
+    lines = [_FOAM_BANNER.rstrip("\n"), "FoamFile", "{", "    version     2.0;", "    format      ascii;",
+             f"    class       {cls};", f'    location    "{location}";', f"    object      {name};", "}",
+             "// * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * //", "",
+             f"dimensions      {dimensions or _DIMENSIONS.get(name, '[0 0 0 0 0 0 0]')}", "", ""]
+    body = _value_block(internal, ncomp, digits, "internalField   ")
+    lines += body
+    lines += ["", "boundaryField", "{"]
+    for pname, ptype, vals in boundary:
+        lines += [f"    {pname}", "    {", f"        type             {ptype};"]
+        if vals is not None:
+            lines += _value_block(vals, ncomp, digits, "        value            ")
+        lines += ["    }"]
+    lines += ["}", ""]
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        f.write("\n".join(lines))
+
+
+def write_time_directory(case_dir: str, time: str, spec, U: np.ndarray, p: np.ndarray, mdot: np.ndarray,
+                         digits: int = 17) -> str:
+    """Checkpoint a steady state: U, p and mdot_f of a case (rows as the C-ABI returns them:
+    U as 3 x (cells + boundary faces), p as cells + boundary faces, mdot per face) into
+    ``case_dir/time`` in OpenFOAM format. Returns the directory."""
+    m = spec.mesh
+    nc, fi = m.n_cells, m.n_interior
+    d = os.path.join(case_dir, time)
+    U = np.asarray(U, dtype=np.float64).reshape(3, -1)
+    p = np.asarray(p, dtype=np.float64).ravel()
+    mdot = np.asarray(mdot, dtype=np.float64).ravel()
+    ub, pb, fb = [], [], []
+    for patch, tu, tp in zip(m.patches, spec.bc_u, spec.bc_p):
+        lo, hi = nc + patch.start - fi, nc + patch.start - fi + patch.n
+        ub.append((patch.name, tu, None if tu == "empty" else U[:, lo:hi].T))
+        pb.append((patch.name, tp, None if tp == "empty" else p[lo:hi]))
+        fb.append((patch.name, "calculated", None if tp == "empty" else mdot[patch.start:patch.start + patch.n]))
+    write_field(os.path.join(d, "U"), "U", "volVectorField", U[:, :nc].T, ub, time, digits=digits)
+    write_field(os.path.join(d, "p"), "p", "volScalarField", p[:nc], pb, time, digits=digits)
+    write_field(os.path.join(d, "mdot_f"), "mdot_f", "surfaceScalarField", mdot[:fi], fb, time, digits=digits)
+    return d
+
+
+def read_time_directory(case_dir: str, time: str, mesh: PolyMesh):
+    """The (U0, p0, mdot0) initial fields of a restart from ``case_dir/time``:
+    U0 (cells, 3), p0 (cells,), mdot0 (faces,) with the boundary faces' mdot from the patches."""
+    d = os.path.join(case_dir, time)
+    fu, fp, fm = read_field(os.path.join(d, "U")), read_field(os.path.join(d, "p")), read_field(os.path.join(d, "mdot_f"))
+    U0 = np.asarray(fu["internal"][1], dtype=np.float64).reshape(-1, 3)
+    p0 = np.asarray(fp["internal"][1], dtype=np.float64).ravel()
+    mdot0 = np.zeros(mesh.n_faces)
+    mdot0[:mesh.n_interior] = np.asarray(fm["internal"][1], dtype=np.float64).ravel()
+    for patch in mesh.patches:
+        ent = fm["boundary"].get(patch.name)
+        if ent and "value" in ent:
+            mdot0[patch.start:patch.start + patch.n] = np.asarray(ent["value"][1], dtype=np.float64).ravel()
+    return U0, p0, mdot0

@@ -198,3 +198,23 @@ def test_full_size_configs_bit_exact(ufvm_mod, oracle_mod, name):
         assert np.allclose(rg[:8], ro[:8], rtol=1e-10, atol=0), (it, rg[:8], ro[:8])
     _compare_case(g, oc, ("U", "p", "mdot"))
     g.close()
+
+
+def test_gpu_restart_from_checkpoint_bit_exact(ufvm_mod, tmp_path):
+    """A GPU case checkpointed to OpenFOAM fields and restarted continues bit for bit."""
+    import dataclasses
+    from matlab_ufvm_b200 import polymesh
+    spec = case.cavity_case(16, nu=0.01)
+    straight = ufvm_mod.GpuCase(spec)
+    for _ in range(5):
+        straight.iterate()
+    first = ufvm_mod.GpuCase(spec)
+    for _ in range(3):
+        first.iterate()
+    polymesh.write_time_directory(str(tmp_path), "3", spec, first.get("U"), first.get("p"), first.get("mdot"))
+    U0, p0, m0 = polymesh.read_time_directory(str(tmp_path), "3", spec.mesh)
+    resumed = ufvm_mod.GpuCase(dataclasses.replace(spec, U0=U0, p0=p0, mdot0=m0))
+    for _ in range(2):
+        resumed.iterate()
+    for name in ("U", "p", "mdot"):
+        same(straight.get(name), resumed.get(name), name)
