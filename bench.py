@@ -507,6 +507,43 @@ def plain_kernel_rooflines(peaks):
     return out
 
 
+def plain_named_configs():
+    """Seconds per steady SIMPLE iteration of the plain FP64 form on the named single-case
+    workloads, on the GPU and in the oracle (one host core), same settings as the reference's
+    tutorials: the 20x20 cavity (Re 100), the 64^3 cavity (Re 400, ILU for p) and the
+    1,029,000-cell jittered-tet channel (Re 200)."""
+    import torch
+    from matlab_ufvm_b200 import case, ufvm
+    from oracle import oracle
+    oracle.build()
+    out = {}
+    for key, make, n_gpu, n_cpu in (
+            ("C1_cavity_20x20", lambda: case.cavity_case(20, nu=0.01), 10, 10),
+            ("C2_cavity_64cubed_ilu", lambda: case.cavity_case(64, nu=1.0 / 400, dim=3, p_smoother="ILU"), 4, 2),
+            ("C3_channel_1M_tet", lambda: case.channel_case(), 3, 1)):
+        spec = make()
+        g = ufvm.GpuCase(spec)
+        g.iterate()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n_gpu):
+            g.iterate()
+        torch.cuda.synchronize()
+        gpu = (time.perf_counter() - t0) / n_gpu
+        g.close()
+        oc = oracle.OracleCase(spec)
+        oc.iterate()
+        t0 = time.perf_counter()
+        for _ in range(n_cpu):
+            oc.iterate()
+        cpu = (time.perf_counter() - t0) / n_cpu
+        del oc
+        out[key] = {"cells": spec.mesh.n_cells, "gpu_ms_per_iteration": round(gpu * 1e3, 3),
+                    "oracle_ms_per_iteration": round(cpu * 1e3, 3), "oracle_cores": 1,
+                    "speedup": round(cpu / gpu, 2)}
+    return out
+
+
 def pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
@@ -591,6 +628,7 @@ def main_ours(args):
         if not args.no_plain:
             plain = plain_gpu_sample(20.0)
             plain["kernels"] = plain_kernel_rooflines(peaks)
+            plain["named"] = plain_named_configs()
         if not args.no_cpu:
             workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
             cpu = cpu_baseline(workers, 2.0)
@@ -622,7 +660,7 @@ def main_ours(args):
                 "method": "plain FP64 form (reference SOR/ILU smoothers, AMG rebuilt every p solve) one case at a "
                           "time: seconds per SIMPLE iteration at n in 16..256 applied to the sweep's iteration counts",
                 "s_per_iter": {str(k): round(s, 6) for k, s in plain["s_per_iter"].items()},
-                "kernels_1M_tet_channel": plain["kernels"]}
+                "kernels_1M_tet_channel": plain["kernels"], "named_configs": plain["named"]}
             line["batched_over_plain"] = value / plain["cases_per_s"] if plain["cases_per_s"] else None
         print(json.dumps(line), flush=True)
     if ws > 1:
