@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-workers", type=int, default=0, help="0: all host cores (at most 64)")
+    ap.add_argument("--profile-plain", choices=("C1", "C2", "C3"), default=None,
+                    help="profiling run for ncu: one plain FP64 SIMPLE iteration of a named single-case "
+                         "workload inside cudaProfilerStart/Stop (after one warm-up iteration)")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: eager launches, warm-up only, then one roofline unit of the "
                          "dominant kernel and one step inside cudaProfilerStart/Stop; prints the unit's bytes")
@@ -322,6 +325,29 @@ def main_profile(args):
     torch.cuda.profiler.stop()
     print(json.dumps({"profile_unit_bytes": by, "profile_unit_ms": ms, "resident": nr}), flush=True)
     svc.close()
+    return 0
+
+
+def main_profile_plain(args):
+    """ncu target: one iteration of the plain FP64 form on a named workload."""
+    import torch
+    from matlab_ufvm_b200 import build as _b, case, ufvm
+    torch.cuda.set_device(0)
+    _b.build()
+    make = {"C1": lambda: case.cavity_case(20, nu=0.01),
+            "C2": lambda: case.cavity_case(64, nu=1.0 / 400, dim=3, p_smoother="ILU"),
+            "C3": lambda: case.channel_case()}[args.profile_plain]
+    g = ufvm.GpuCase(make())
+    g.iterate()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    t0 = time.perf_counter()
+    g.iterate()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    torch.cuda.profiler.stop()
+    print(json.dumps({"plain_iteration_s": el, "workload": args.profile_plain}), flush=True)
+    g.close()
     return 0
 
 
@@ -675,6 +701,8 @@ def main():
         return main_reference(args)
     if args.profile:
         return main_profile(args)
+    if args.profile_plain:
+        return main_profile_plain(args)
     return main_ours(args)
 
 

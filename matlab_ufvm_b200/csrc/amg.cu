@@ -14,6 +14,7 @@
 // Claim sets only shrink as cells get assigned, so a committed seed's claims are the
 // ones it would make in the sequential sweep, and the final `parents` map is identical.
 // Orphans are attached in rounds that respect their natural-order dependencies.
+#include <atomic>
 #include "amg.cuh"
 
 namespace ufvm {
@@ -402,7 +403,7 @@ int AmgSolver::build(std::vector<Level>& lev, int max_coarse, int quirks, int* n
 
 void free_level(Level& L, bool keep_matrix) {
   if (!keep_matrix) { dfree(L.rowptr); dfree(L.col); dfree(L.ac); dfree(L.anb); dfree(L.bc); dfree(L.dphi); }
-  dfree(L.parents); dfree(L.tpos); dfree(L.r); dfree(L.dc); dfree(L.rc); dfree(L.lvl); dfree(L.fwdRows);
+  dfree(L.parents); dfree(L.tpos); dfree(L.lord); dfree(L.r); dfree(L.dc); dfree(L.rc); dfree(L.lvl); dfree(L.fwdRows);
   dfree(L.fwdStart); dfree(L.bwdRows); dfree(L.bwdStart); dfree(L.color); dfree(L.colorRows); dfree(L.colorStart);
   dfree(L.childStart); dfree(L.child); dfree(L.ac32); dfree(L.anb32); dfree(L.bc32); dfree(L.dphi32); dfree(L.r32);
   dfree(L.fr); dfree(L.fp); dfree(L.fq);
@@ -411,6 +412,7 @@ void free_level(Level& L, bool keep_matrix) {
   L.ell_valid = false;
   L.sched_valid = false;
   L.color_valid = false;
+  L.dc_epoch = 0;
 }
 
 int AmgSolver::smooth(std::vector<Level>& lev, int l, int n_iter, double rrf) {
@@ -468,6 +470,14 @@ int AmgSolver::apply(std::vector<Level>& lev, bool rebuild, int* n_levels, doubl
   UFVM_CHECK(sum_abs_residual(ctx, lev[0], lev[0].dphi.p, &init));
   double fin = init;
   int ncyc = 1;
+  // the matrices are final from here to the end of this solve: a fresh epoch lets the smoother
+  // calls of the cycles share each level's DILU factor
+  static std::atomic<unsigned long long> epochs{0};
+  struct EpochScope {
+    LinCtx& c;
+    ~EpochScope() { c.factor_epoch = 0; }
+  } scope{ctx};
+  ctx.factor_epoch = epochs.fetch_add(1) + 1;
   while (ncyc <= max_cycles && fin > rrf * init) {
     UFVM_CHECK(cycle(lev, L, rrf, &fin));
     ++ncyc;

@@ -33,10 +33,14 @@ struct Level {
   int n = 0, nnz = 0;
   DArr<int> rowptr, col, parents, tpos;
   DArr<double> ac, anb, bc, dphi, r, dc, rc;
-  // level schedules for the natural-order sweeps
+  // level schedules for the natural-order sweeps; lord lists each row's lower neighbours as
+  // CSR positions in increasing column order (-1 in the row's remaining slots)
   bool sched_valid = false;
   int nfwd = 0, nbwd = 0, maxw = 0;
-  DArr<int> lvl, fwdRows, fwdStart, bwdRows, bwdStart;
+  DArr<int> lvl, fwdRows, fwdStart, bwdRows, bwdStart, lord;
+  // dc holds the DILU factor of the current matrix while dc_epoch equals the solver's epoch
+  unsigned long long dc_epoch = 0;
+  int dc_quirks = 0;
   // multicolour ordering
   bool color_valid = false;
   int ncolor = 0;
@@ -69,6 +73,11 @@ struct LinCtx {
   DArr<int> iflag, iscan;      // flags / scan temporaries
   DArr<unsigned int> bar;      // grid barrier: count, gen
   DArr<int> berr;              // grid barrier timeout flag
+  // An AMG solve keeps every level's matrix fixed, so the DILU factor computed by the first
+  // smoother call on a level is reused by the later ones of the same solve (the factorisation
+  // is a function of the matrix alone: same bits). factor_epoch names the solve; 0 = no reuse.
+  unsigned long long factor_epoch = 0;
+  int cluster_ok = 0;  // cluster sweeps: 0 not yet probed, 1 usable, -1 not usable
   int ensure(int n);
   void release();
 };

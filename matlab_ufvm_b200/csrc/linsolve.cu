@@ -276,6 +276,27 @@ int build_tpos(LinCtx& c, Level& L) {
   return UFVM_OK;
 }
 
+// lord: for each row, the CSR positions of its lower neighbours in increasing column order
+// (the order in which the reference's outer loop over i1 delivers them), then -1 in the row's
+// remaining slots. Built once per pattern by repeated minimum search.
+__global__ void k_lower_order(int n, const int* __restrict__ rp, const int* __restrict__ col, int* lord) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k0 = rp[i], k1 = rp[i + 1];
+  int t = k0, prev = -1;
+  while (true) {
+    int best = 0x7fffffff, bk = -1;
+    for (int k = k0; k < k1; ++k) {
+      const int j = col[k];
+      if (j < i && j > prev && j < best) { best = j; bk = k; }
+    }
+    if (bk < 0) break;
+    prev = best;
+    lord[t++] = bk;
+  }
+  for (; t < k1; ++t) lord[t] = -1;
+}
+
 int build_schedule(LinCtx& c, Level& L) {
   if (L.sched_valid) return UFVM_OK;
   UFVM_CHECK(c.ensure(L.n));
@@ -283,7 +304,11 @@ int build_schedule(LinCtx& c, Level& L) {
   UFVM_CHECK(one_schedule(c, L, true, L.fwdRows, L.fwdStart, L.nfwd));
   UFVM_CHECK(one_schedule(c, L, false, L.bwdRows, L.bwdStart, L.nbwd));
   UFVM_CHECK(build_tpos(c, L));
+  UFVM_CHECK(dalloc(L.lord, std::max(L.nnz, 1)));
+  k_lower_order<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.lord.p);
+  UFVM_LAUNCH_CHECK();
   L.sched_valid = true;
+  L.dc_epoch = 0;
   return UFVM_OK;
 }
 
@@ -292,59 +317,97 @@ enum { OP_GS = 0, OP_ILU_FACT = 1, OP_ILU_FWD = 2, OP_ILU_BWD = 3 };
 
 struct SweepArgs {
   int n, nlev, quirks;
-  const int *lstart, *rows, *rp, *col, *tpos;
+  const int *lstart, *rows, *rp, *col, *tpos, *lord;
   const double *ac, *anb, *bc;
   double *x, *dc, *rc;
 };
 
-// Lower neighbours of row j in increasing column order (the order in which the
-// reference's outer loop over i1 delivers them), visited by repeated minimum search.
+// One row of a sweep, with the reference's operation order. The products that a row
+// subtracts do not depend on one another, so they are formed kChunk at a time (their loads
+// in flight together) and then subtracted one by one in the reference's order: the same
+// operations on the same operands, so the same bits.
+constexpr int kChunk = 8;
+
 template <int OP>
 __device__ __forceinline__ void row_op(int i, const SweepArgs& a) {
   const int k0 = a.rp[i], k1 = a.rp[i + 1];
   if (OP == OP_GS) {
+    // solve/cfdSolveSOR.m:13-29: v = bc - sum anb * x in cconn order, x = v / ac
     double v = a.bc[i];
-    for (int k = k0; k < k1; ++k) v = v - a.anb[k] * __ldcg(a.x + a.col[k]);
+    for (int k = k0; k < k1; k += kChunk) {
+      double p[kChunk];
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t) p[t] = k + t < k1 ? a.anb[k + t] * __ldcg(a.x + a.col[k + t]) : 0.0;
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t)
+        if (k + t < k1) v = v - p[t];
+    }
     __stcg(a.x + i, v / a.ac[i]);
   } else if (OP == OP_ILU_FACT) {
+    // solve/cfdFactorizeILU.m:5-47: d = ac - sum over lower j (increasing) of anb(i,j) dc_j anb(j,i)
     double d = a.ac[i];
-    int prev = -1;
-    while (true) {
-      int best = 0x7fffffff, bk = -1;
-      for (int k = k0; k < k1; ++k) {
-        const int j = a.col[k];
-        if (j < i && j > prev && j < best) { best = j; bk = k; }
+    for (int k = k0; k < k1; k += kChunk) {
+      double p[kChunk];
+      bool use[kChunk];
+      bool done = false;
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t) {
+        const int q = k + t < k1 ? a.lord[k + t] : -1;
+        done |= q < 0;
+        int j = q >= 0 ? a.col[q] : -1;
+        // Q7: the reference's factorisation loop skips row N-1 (1-based), i.e. row n-2
+        const bool skip = (a.quirks & UFVM_Q7_ILU_SKIP_ROW) && j == a.n - 2;
+        const int tk = q >= 0 ? a.tpos[q] : -1;  // the pattern is structurally symmetric, so tk >= 0
+        use[t] = q >= 0 && !skip && tk >= 0;
+        p[t] = use[t] ? a.anb[q] * __ldcg(a.dc + j) * a.anb[tk] : 0.0;
       }
-      if (bk < 0) break;
-      prev = best;
-      // Q7: the reference's factorisation loop skips row N-1 (1-based), i.e. row n-2
-      if ((a.quirks & UFVM_Q7_ILU_SKIP_ROW) && best == a.n - 2) continue;
-      const int tk = a.tpos[bk];  // the pattern is structurally symmetric, so tk >= 0
-      if (tk >= 0) d = d - a.anb[bk] * __ldcg(a.dc + best) * a.anb[tk];
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t)
+        if (use[t]) d = d - p[t];
+      if (done) break;
     }
     __stcg(a.dc + i, 1.0 / d);
   } else if (OP == OP_ILU_FWD) {
+    // solve/cfdSolveILU.m forward substitution over lower j in increasing order
     double v = __ldcg(a.rc + i);
-    int prev = -1;
-    while (true) {
-      int best = 0x7fffffff, bk = -1;
-      for (int k = k0; k < k1; ++k) {
-        const int j = a.col[k];
-        if (j < i && j > prev && j < best) { best = j; bk = k; }
+    for (int k = k0; k < k1; k += kChunk) {
+      double p[kChunk];
+      bool use[kChunk];
+      bool done = false;
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t) {
+        const int q = k + t < k1 ? a.lord[k + t] : -1;
+        done |= q < 0;
+        use[t] = q >= 0;
+        if (use[t]) {
+          const int j = a.col[q];
+          const double mat1 = __ldcg(a.dc + j) * __ldcg(a.rc + j);
+          p[t] = a.anb[q] * mat1;
+        } else {
+          p[t] = 0.0;
+        }
       }
-      if (bk < 0) break;
-      prev = best;
-      const double mat1 = __ldcg(a.dc + best) * __ldcg(a.rc + best);
-      const double mat2 = a.anb[bk] * mat1;
-      v = v - mat2;
+#pragma unroll
+      for (int t = 0; t < kChunk; ++t)
+        if (use[t]) v = v - p[t];
+      if (done) break;
     }
     __stcg(a.rc + i, v);
-  } else {  // OP_ILU_BWD
+  } else {  // OP_ILU_BWD: backward substitution over upper j in cconn order, then the update
     double v = __ldcg(a.rc + i);
     if (i < a.n - 1) {
-      for (int k = k0; k < k1; ++k) {
-        const int j = a.col[k];
-        if (j > i) v = v - a.anb[k] * __ldcg(a.rc + j);
+      for (int k = k0; k < k1; k += kChunk) {
+        double p[kChunk];
+        bool use[kChunk];
+#pragma unroll
+        for (int t = 0; t < kChunk; ++t) {
+          const int j = k + t < k1 ? a.col[k + t] : -1;
+          use[t] = j > i;
+          p[t] = use[t] ? a.anb[k + t] * __ldcg(a.rc + j) : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < kChunk; ++t)
+          if (use[t]) v = v - p[t];
       }
     }
     const double mat1 = __ldcg(a.dc + i) * v;
@@ -353,6 +416,7 @@ __device__ __forceinline__ void row_op(int i, const SweepArgs& a) {
   }
 }
 
+// Wide schedules: one cooperative grid, a software grid barrier between dependency levels.
 template <int OP>
 __global__ void k_sched_sweep(SweepArgs a, GridBarrier bar) {
   unsigned int gen = grid_gen0(bar);
@@ -362,6 +426,34 @@ __global__ void k_sched_sweep(SweepArgs a, GridBarrier bar) {
     for (int idx = s + tid; idx < e; idx += nth) row_op<OP>(a.rows[idx], a);
     if (L + 1 < a.nlev)
       if (!grid_sync(bar, gen)) return;
+  }
+}
+
+// Narrow schedules (every level at most a few thousand rows, as in the natural-order sweeps
+// of structured meshes and of every coarse AMG level): one CTA, or one thread-block cluster
+// of up to 8 CTAs, with the hardware barrier between levels. Writes of a level are made at
+// L2 (st.global.cg) and read back from L2 (ld.global.cg); the CTA barrier, or the cluster
+// barrier's release/acquire pair, orders them. Every thread of every CTA executes every
+// barrier (no early exit), so the barrier cannot wait on a missing CTA.
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;\n" ::: "memory");
+}
+
+template <int OP, bool CLUSTER>
+__global__ void __launch_bounds__(1024) k_sched_sweep_cl(SweepArgs a) {
+  unsigned int rank = 0, size = 1;
+  if (CLUSTER) {
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(size));
+  }
+  const int tid = (int)rank * blockDim.x + threadIdx.x, nth = (int)size * blockDim.x;
+  for (int L = 0; L < a.nlev; ++L) {
+    const int s = a.lstart[L], e = a.lstart[L + 1];
+    for (int idx = s + tid; idx < e; idx += nth) row_op<OP>(a.rows[idx], a);
+    if (L + 1 < a.nlev) {
+      if (CLUSTER) cluster_barrier();
+      else __syncthreads();
+    }
   }
 }
 
@@ -376,6 +468,9 @@ __global__ void k_ilu_res(int n, const int* __restrict__ rp, const int* __restri
   rc[i] = res;
 }
 
+// Rows a cluster sweep handles per thread and level before the wide (grid) form pays off.
+constexpr int kClusterRowsPerThread = 4;
+
 template <int OP>
 static int launch_sweep(LinCtx& c, Level& L, bool fwd, int quirks) {
   SweepArgs a;
@@ -383,9 +478,48 @@ static int launch_sweep(LinCtx& c, Level& L, bool fwd, int quirks) {
   a.nlev = fwd ? L.nfwd : L.nbwd;
   a.lstart = fwd ? L.fwdStart.p : L.bwdStart.p;
   a.rows = fwd ? L.fwdRows.p : L.bwdRows.p;
-  a.rp = L.rowptr.p; a.col = L.col.p; a.tpos = L.tpos.p;
+  a.rp = L.rowptr.p; a.col = L.col.p; a.tpos = L.tpos.p; a.lord = L.lord.p;
   a.ac = L.ac.p; a.anb = L.anb.p; a.bc = L.bc.p;
   a.x = L.dphi.p; a.dc = L.dc.p; a.rc = L.rc.p;
+  const int w = std::max(L.maxw, 1);
+  if (w <= 1024) {
+    const int bs = std::min(1024, std::max(32, (w + 31) / 32 * 32));
+    k_sched_sweep_cl<OP, false><<<1, bs, 0, c.stream>>>(a);
+    UFVM_LAUNCH_CHECK();
+    return UFVM_OK;
+  }
+  if (w <= 8 * 1024 * kClusterRowsPerThread && c.cluster_ok >= 0) {
+    int cs = 2;
+    while (cs < 8 && cs * 1024 < w) cs *= 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (c.cluster_ok == 0) {
+      // once per context: can a cluster of 8 such CTAs be resident?
+      int ncl = 0;
+      cudaLaunchConfig_t q = cfg;
+      q.gridDim = dim3(8);
+      cudaLaunchAttribute qa[1] = {attr[0]};
+      qa[0].val.clusterDim.x = 8;
+      q.attrs = qa;
+      const cudaError_t e = cudaOccupancyMaxActiveClusters(&ncl, (const void*)k_sched_sweep_cl<OP, true>, &q);
+      if (e != cudaSuccess) (void)cudaGetLastError();
+      c.cluster_ok = (e == cudaSuccess && ncl >= 1) ? 1 : -1;
+    }
+    if (c.cluster_ok > 0) {
+      UFVM_CUDA(cudaLaunchKernelEx(&cfg, k_sched_sweep_cl<OP, true>, a));
+      return UFVM_OK;
+    }
+  }
   GridBarrier gb{c.bar.p, c.bar.p + 1, c.berr.p};
   int maxb = 0;
   UFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, k_sched_sweep<OP>, kBlock, 0));
@@ -420,8 +554,13 @@ int gs_sweep(LinCtx& c, Level& L) {
 int ilu_factor(LinCtx& c, Level& L, int quirks) {
   UFVM_CHECK(c.ensure(L.n));
   UFVM_CHECK(build_schedule(c, L));
+  // within one AMG solve the level's matrix is fixed: the factor already computed is the one
+  // the reference recomputes on every smoother call
+  if (c.factor_epoch != 0 && L.dc_epoch == c.factor_epoch && L.dc_quirks == quirks && L.dc.p) return UFVM_OK;
   UFVM_CHECK(dalloc(L.dc, L.n));
   UFVM_CHECK(launch_sweep<OP_ILU_FACT>(c, L, true, quirks));
+  L.dc_epoch = c.factor_epoch;
+  L.dc_quirks = quirks;
   return UFVM_OK;
 }
 
