@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--profile-plain", choices=("C1", "C2", "C3"), default=None,
                     help="profiling run for ncu: one plain FP64 SIMPLE iteration of a named single-case "
                          "workload inside cudaProfilerStart/Stop (after one warm-up iteration)")
+    ap.add_argument("--plain-kernels", action="store_true",
+                    help="only the plain FP64 form's solver-kernel rooflines on the 1M-cell tet channel (one JSON "
+                         "line per kernel; the ncu target for those kernels)")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: eager launches, warm-up only, then one roofline unit of the "
                          "dominant kernel and one step inside cudaProfilerStart/Stop; prints the unit's bytes")
@@ -483,49 +486,31 @@ def plain_gpu_sample(budget_s: float):
 
 
 def plain_kernel_rooflines(peaks):
-    """The plain FP64 form's residual array and SOR sweep on the 1,029,000-cell tet channel's
-    momentum matrix (device pointers through the C-ABI), L2 flushed before every launch."""
-    import ctypes as ct
+    """The plain FP64 form's solver kernels on the 1,029,000-cell tet channel's momentum matrix
+    (device arrays), kernel time only: the library's profiling entry point prepares schedules,
+    colourings and the DILU factor, then times each launch with CUDA events after a read of
+    twice the L2 size."""
     import torch
     from matlab_ufvm_b200 import case, ufvm
     spec = case.channel_case()
     g = ufvm.GpuCase(spec)
-    g.iterate()  # builds the level structure once
+    g.iterate()
     g.cfdUpdateFields()
     g.cfdAssembleEquation("U", 1)
-    rp = torch.from_numpy(g.level_array(0, "rowptr")).cuda()
-    col = torch.from_numpy(g.level_array(0, "col")).cuda()
-    ac = torch.from_numpy(g.get("ac")).cuda()
-    anb = torch.from_numpy(g.get("anb")).cuda()
-    bc = torch.from_numpy(g.get("bc")).cuda()
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda()
+           for a in (g.level_array(0, "rowptr"), g.level_array(0, "col"), g.get("ac"), g.get("anb"), g.get("bc"))]
     g.close()
-    n, nnz = ac.numel(), anb.numel()
-    x = torch.randn(n, dtype=torch.float64, device="cuda")
-    r = torch.empty_like(x)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
-    lib = ufvm.lib()
-    st = torch.cuda.current_stream()
-    P = lambda t: ct.c_void_p(t.data_ptr())
+    n, nnz = dev[2].numel(), dev[3].numel()
     out = []
-    for name, call, by in (
-            ("k_residual (plain FP64 r = b - A x, cfdComputeResidualsArray)",
-             lambda: lib.ufvm_compute_residuals_array(n, P(rp), P(col), P(ac), P(anb), P(bc), P(x), P(r),
-                                                      ct.c_void_p(st.cuda_stream)),
-             36.0 * n + 12.0 * nnz),
-            ("k_sched_sweep<GS> (plain FP64 symmetric natural-order Gauss-Seidel, level scheduled, cfdSolveSOR)",
-             lambda: lib.ufvm_solve_sor(n, P(rp), P(col), P(ac), P(anb), P(bc), P(x), ct.c_void_p(st.cuda_stream)),
-             2.0 * (36.0 * n + 12.0 * nnz))):
-        assert call() == 0
-        times = []
-        for _ in range(5):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            assert call() == 0
-            e1.record(st)
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
-        ms = statistics.median(times)
+    for key, name in (
+            ("residual", "k_residual (plain FP64 r = b - A x, cfdComputeResidualsArray)"),
+            ("MCGS", "k_mc_rows (plain FP64 symmetric multicolour Gauss-Seidel, colour-major ELL copy)"),
+            ("SOR", "k_sched_sweep_cl (plain FP64 symmetric natural-order Gauss-Seidel, level scheduled, "
+                    "cfdSolveSOR: latency-bound by its dependency levels)"),
+            ("ILU", "k_ilu_res + k_sched_sweep_cl (plain FP64 DILU application, level scheduled, cfdSolveILU: "
+                    "latency-bound by its dependency levels)")):
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ms, by = ufvm.profile_plain_kernel(key, *dev, x, 5)
         a = by / (ms * 1e-3) / 1e9
         out.append({"kernel": name, "rows": n, "nnz": nnz, "bytes": by, "ms": round(ms, 4),
                     "achieved": round(a, 1), "unit": "GB/s",
@@ -703,6 +688,14 @@ def main():
         return main_profile(args)
     if args.profile_plain:
         return main_profile_plain(args)
+    if args.plain_kernels:
+        import torch
+        from matlab_ufvm_b200 import build as _b
+        torch.cuda.set_device(0)
+        _b.build()
+        for row in plain_kernel_rooflines(load_peaks()):
+            print(json.dumps(row), flush=True)
+        return 0
     return main_ours(args)
 
 

@@ -189,6 +189,20 @@ int ufvm_solve_algebraic_system(int32_t n, const int32_t* rowptr, const int32_t*
                                 double* dphi, int32_t smoother, int32_t n_iter, double rrf,
                                 int32_t quirks, double* r0, double* r1, int32_t* iters,
                                 void* stream);
+/* Kernel timing of the stand-alone solver kernels on one system (no reference counterpart:
+ * the measurement behind the plain form's roofline). kernel 0: residual r = b - A x;
+ * 1: one symmetric natural-order Gauss-Seidel sweep (level scheduled, as ufvm_solve_sor);
+ * 2: one symmetric multicolour Gauss-Seidel sweep (smoother UFVM_SMOOTHER_MCGS);
+ * 3: one DILU application (as ufvm_solve_ilu, factor prepared untimed). Schedules, colourings
+ * and the factor are built first and one launch is made untimed; each of the reps timed
+ * launches follows a read of twice the L2 size and is bracketed by CUDA events on the stream.
+ * ms_per_launch: mean time; bytes_per_launch: algorithmic bytes (36 n + 12 nnz per pass over
+ * the system; 2 passes for a symmetric sweep; DILU adds 40 n + 24 nnz). Sweeps overwrite dphi;
+ * the call allocates (L2-flush buffer and the schedules). */
+int ufvm_profile_plain_kernel(int32_t kernel, int32_t n, const int32_t* rowptr, const int32_t* col,
+                              const double* ac, const double* anb, const double* bc, double* dphi,
+                              int32_t reps, double* ms_per_launch, double* bytes_per_launch,
+                              void* stream);
 /* One level of cfdAgglomerateLevel + assembleAgglomeratedLHS (device pointers in, host
  * count out). parents[n]; coarse rowptr[n+1], col/anb capacity rowptr[n] entries, ac[n]. */
 int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col,

@@ -353,6 +353,7 @@ int agglomerate_level(LinCtx& c, AggScratch& w, Level& F, Level& C, int* nCoarse
   UFVM_CUDA(cudaMemsetAsync(C.dphi.p, 0, nc * sizeof(double), st));
   C.sched_valid = false;
   C.color_valid = false;
+  C.mc_valid = false;
   return galerkin(c, F, C);
 }
 
@@ -409,6 +410,9 @@ void free_level(Level& L, bool keep_matrix) {
   dfree(L.fr); dfree(L.fp); dfree(L.fq);
   dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.childStartP); dfree(L.gpos);
   dfree(L.ellAnb); dfree(L.uAnb); dfree(L.uAc); dfree(L.uBc); dfree(L.uX);
+  dfree(L.mcRow); dfree(L.mcCol); dfree(L.mcAnb); dfree(L.mcAc); dfree(L.mcBc);
+  L.mc_valid = false;
+  L.mc_epoch = 0;
   L.ell_valid = false;
   L.sched_valid = false;
   L.color_valid = false;

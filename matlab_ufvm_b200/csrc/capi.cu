@@ -437,6 +437,92 @@ int ufvm_solve_algebraic_system(int32_t n, const int32_t* rowptr, const int32_t*
   return st;
 }
 
+// Profiling of the stand-alone kernels: schedules, colourings and factors are prepared and
+// one launch is made untimed; then every timed launch follows a read of twice the L2 size (the
+// cache holds clean unrelated lines, nothing of the system and nothing dirty) and is bracketed
+// by CUDA events on the caller's stream.
+__global__ void k_flush_read(const float4* __restrict__ a, size_t n4, float* sink) {
+  float s = 0.f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    const float4 v = a[i];
+    s += v.x + v.y + v.z + v.w;
+  }
+  if (s == 1.2345e-30f) *sink = s;  // never true for the zeroed buffer; keeps the loads
+}
+
+int ufvm_profile_plain_kernel(int32_t kernel, int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
+                              const double* anb, const double* bc, double* dphi, int32_t reps, double* ms_per_launch,
+                              double* bytes_per_launch, void* stream) {
+  if (n <= 0 || !rowptr || !col || !ac || !anb || !bc || !dphi || reps <= 0 || !ms_per_launch || !bytes_per_launch ||
+      kernel < 0 || kernel > 3) {
+    set_error("ufvm_profile_plain_kernel: bad argument");
+    return UFVM_E_INVALID;
+  }
+  LinCtx c;
+  c.stream = (cudaStream_t)stream;
+  int dev = 0;
+  UFVM_CUDA(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, dev);
+  int l2 = 0;
+  cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+  int nnz = 0;
+  UFVM_CHECK(nnz_of(n, rowptr, c.stream, &nnz));
+  Level L = borrow(n, rowptr, col, ac, anb, bc, dphi, nnz);
+  DArr<double> r;
+  DArr<float4> flush;
+  DArr<float> sink;
+  cudaEvent_t a = nullptr, b = nullptr;
+  auto body = [&]() -> int {
+    const size_t n4 = std::max<size_t>(2 * (size_t)std::max(l2, 1 << 20) / sizeof(float4), 1);
+    UFVM_CHECK(dalloc(flush, n4));
+    UFVM_CHECK(dalloc(sink, 1));
+    UFVM_CUDA(cudaMemsetAsync(flush.p, 0, n4 * sizeof(float4), c.stream));
+    UFVM_CHECK(c.ensure(n));
+    if (kernel == 0) UFVM_CHECK(dalloc(r, n));
+    if (kernel == 1 || kernel == 3) UFVM_CHECK(build_schedule(c, L));
+    if (kernel == 2) UFVM_CHECK(mcgs_prepare(c, L));
+    if (kernel == 3) {
+      UFVM_CHECK(ilu_factor(c, L, 0));
+    }
+    auto unit = [&]() -> int {
+      if (kernel == 0) return residual(c, L, L.dphi.p, r.p);
+      if (kernel == 1) return gs_sweep(c, L);
+      if (kernel == 2) return mcgs_sweep(c, L);
+      return ilu_sweep(c, L);
+    };
+    UFVM_CHECK(unit());
+    UFVM_CUDA(cudaEventCreate(&a));
+    UFVM_CUDA(cudaEventCreate(&b));
+    double total = 0;
+    for (int k = 0; k < reps; ++k) {
+      k_flush_read<<<4 * c.nsm, 512, 0, c.stream>>>(flush.p, n4, sink.p);
+      UFVM_LAUNCH_CHECK();
+      UFVM_CUDA(cudaEventRecord(a, c.stream));
+      UFVM_CHECK(unit());
+      UFVM_CUDA(cudaEventRecord(b, c.stream));
+      UFVM_CUDA(cudaEventSynchronize(b));
+      float t = 0;
+      UFVM_CUDA(cudaEventElapsedTime(&t, a, b));
+      total += t;
+    }
+    if (kernel == 1 || kernel == 3) UFVM_CHECK(check_barrier(c));
+    *ms_per_launch = total / reps;
+    const double pass = 36.0 * n + 12.0 * nnz;  // one read of the system and x, one vector written
+    *bytes_per_launch = kernel == 0 ? pass : kernel == 3 ? pass + 40.0 * n + 24.0 * nnz : 2.0 * pass;
+    return UFVM_OK;
+  };
+  const int st = body();
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaStreamSynchronize(c.stream);
+  dfree(flush);
+  dfree(sink);
+  dfree(r);
+  unborrow(L);
+  c.release();
+  return st;
+}
+
 int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac, const double* anb,
                            int32_t* parents, int32_t* c_rowptr, int32_t* c_col, double* c_ac, double* c_anb,
                            int32_t* n_coarse, int32_t* nnz_coarse, void* stream) {

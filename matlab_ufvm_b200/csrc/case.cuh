@@ -46,6 +46,14 @@ struct Level {
   int ncolor = 0;
   DArr<int> color, colorRows, colorStart;
   std::vector<int> h_colorStart;
+  // colour-major ELL copy for the plain FP64 multicolour sweep: position p holds row mcRow[p]
+  // (colours ascending, rows ascending inside a colour), entry k at [k * n + p]; mc_epoch as
+  // dc_epoch for the copied matrix values
+  bool mc_valid = false;
+  int mcW = 0;
+  unsigned long long mc_epoch = 0;
+  DArr<int> mcRow, mcCol;
+  DArr<double> mcAnb, mcAc, mcBc;
   // children of each coarse row of the NEXT level (restriction / Galerkin)
   DArr<int> childStart, child;
   // FP32 copies for the mixed-precision smoother

@@ -96,48 +96,37 @@ int scan_exclusive(LinCtx& c, const int* in, int* out, int n, int* total_host) {
 }
 
 // ---------------------------------------------------------------- residual
-// The block's rows own one contiguous range of the CSR arrays. It is staged through shared
-// memory with unit-stride loads by the whole block (kStageEntries entries at most; a longer
-// range is read directly), then each thread sums its own row from shared memory in the
-// cconn order, so the result is the same bit for bit as the direct per-row loop.
-constexpr int kStageEntries = 8 * kBlock;
+// One row per thread. Everything a row needs apart from the neighbour values (its row
+// pointers, bc, ac, x_i) is loaded at once, then its entries kResChunk at a time (the L1
+// serves the warp's neighbouring rows from the same sectors), then the neighbour values:
+// three dependent memory round trips per row. v = bc - ac x_i, then v = v - anb x_j in cconn
+// order, with each product rounded before the subtraction as in the sequential loop.
+constexpr int kResChunk = 4;
+constexpr int kResBlock = 128;
 
-__device__ __forceinline__ double block_row_residual(int n, const int* __restrict__ rp, const int* __restrict__ col,
-                                                     const double* __restrict__ ac, const double* __restrict__ anb,
-                                                     const double* __restrict__ bc, const double* __restrict__ x,
-                                                     double* s_anb, int* s_col, bool* valid) {
-  const int r0 = blockIdx.x * blockDim.x;
-  const int r1 = min(n, r0 + (int)blockDim.x);
-  const int k0 = rp[r0], k1 = rp[r1];
-  const bool staged = k1 - k0 <= kStageEntries;  // uniform across the block
-  if (staged) {
-    for (int k = k0 + (int)threadIdx.x; k < k1; k += blockDim.x) {
-      s_anb[k - k0] = anb[k];
-      s_col[k - k0] = col[k];
-    }
-  }
-  __syncthreads();
-  const int i = r0 + threadIdx.x;
-  *valid = i < n;
-  if (i >= n) return 0.0;
+__device__ __forceinline__ double row_residual(int i, const int* __restrict__ rp, const int* __restrict__ col,
+                                               const double* __restrict__ ac, const double* __restrict__ anb,
+                                               const double* __restrict__ bc, const double* __restrict__ x) {
+  const int k0 = rp[i], k1 = rp[i + 1];
   double v = bc[i] - ac[i] * x[i];
-  if (staged) {
-    for (int k = rp[i] - k0; k < rp[i + 1] - k0; ++k) v = v - s_anb[k] * x[s_col[k]];
-  } else {
-    for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - anb[k] * x[col[k]];
+  for (int k = k0; k < k1; k += kResChunk) {
+    double p[kResChunk];
+#pragma unroll
+    for (int t = 0; t < kResChunk; ++t) p[t] = k + t < k1 ? anb[k + t] * x[col[k + t]] : 0.0;
+#pragma unroll
+    for (int t = 0; t < kResChunk; ++t)
+      if (k + t < k1) v = v - p[t];
   }
   return v;
 }
 
-__global__ void __launch_bounds__(kBlock) k_residual(int n, const int* __restrict__ rp, const int* __restrict__ col,
-                                                     const double* __restrict__ ac, const double* __restrict__ anb,
-                                                     const double* __restrict__ bc, const double* __restrict__ x,
-                                                     double* __restrict__ r) {
-  __shared__ double s_anb[kStageEntries];
-  __shared__ int s_col[kStageEntries];
-  bool valid;
-  const double v = block_row_residual(n, rp, col, ac, anb, bc, x, s_anb, s_col, &valid);
-  if (valid) r[blockIdx.x * blockDim.x + threadIdx.x] = v;
+__global__ void __launch_bounds__(kResBlock) k_residual(int n, const int* __restrict__ rp,
+                                                        const int* __restrict__ col, const double* __restrict__ ac,
+                                                        const double* __restrict__ anb,
+                                                        const double* __restrict__ bc,
+                                                        const double* __restrict__ x, double* __restrict__ r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = row_residual(i, rp, col, ac, anb, bc, x);
 }
 
 // sum_i |r_i| : block partials (stage 1)
@@ -145,12 +134,9 @@ __global__ void __launch_bounds__(kBlock) k_sumabs_res(int n, const int* __restr
                                                        const double* __restrict__ ac, const double* __restrict__ anb,
                                                        const double* __restrict__ bc, const double* __restrict__ x,
                                                        double* part) {
-  __shared__ double s_anb[kStageEntries];
-  __shared__ int s_col[kStageEntries];
   __shared__ double sh[32];
-  bool valid;
-  const double r = block_row_residual(n, rp, col, ac, anb, bc, x, s_anb, s_col, &valid);
-  double v = valid ? fabs(r) : 0.0;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = i < n ? fabs(row_residual(i, rp, col, ac, anb, bc, x)) : 0.0;
   v = block_reduce<0>(v, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
@@ -165,7 +151,8 @@ __global__ void k_sum_partials(int np, const double* __restrict__ part, double* 
 }
 
 int residual(LinCtx& c, const Level& L, const double* x, double* r) {
-  k_residual<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.ac.p, L.anb.p, L.bc.p, x, r);
+  k_residual<<<nblocks(L.n, kResBlock), kResBlock, 0, c.stream>>>(L.n, L.rowptr.p, L.col.p, L.ac.p, L.anb.p,
+                                                                   L.bc.p, x, r);
   UFVM_LAUNCH_CHECK();
   return UFVM_OK;
 }
@@ -530,7 +517,7 @@ static int launch_sweep(LinCtx& c, Level& L, bool fwd, int quirks) {
   return UFVM_OK;
 }
 
-static int check_barrier(LinCtx& c) {
+int check_barrier(LinCtx& c) {
   int err = 0;
   UFVM_CUDA(cudaMemcpyAsync(&err, c.berr.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   UFVM_CUDA(cudaStreamSynchronize(c.stream));
@@ -657,29 +644,170 @@ int build_coloring(LinCtx& c, Level& L) {
   return UFVM_OK;
 }
 
-__global__ void k_gs_rows(int cnt, const int* __restrict__ rows, const int* __restrict__ rp, const int* __restrict__ col,
-                          const double* __restrict__ ac, const double* __restrict__ anb, const double* __restrict__ bc,
-                          double* x) {
+// The plain FP64 multicolour sweep reads a colour-major ELL copy of the matrix: position p
+// holds row mcRow[p] (colours ascending, rows ascending inside a colour), entry k of position
+// p sits at [k * n + p] (column -1 past the row's end), so a colour's rows are read with
+// unit stride. x stays in natural order. Each row evaluates v = bc - sum anb * x in cconn
+// order and x = v / ac, the operation order of the CSR sweep: the copy changes no bit.
+__global__ void k_color_flag(int n, const int* __restrict__ color, int c, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = color[i] == c;
+}
+
+__global__ void k_color_place(int n, const int* __restrict__ color, int c, int base, const int* __restrict__ pos,
+                              int* mcRow) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && color[i] == c) mcRow[base + pos[i]] = i;
+}
+
+__global__ void k_row_len_max(int n, const int* __restrict__ rp, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicMax(out, rp[i + 1] - rp[i]);
+}
+
+__global__ void k_mc_pattern(int n, int W, const int* __restrict__ mcRow, const int* __restrict__ rp,
+                             const int* __restrict__ col, int* mcCol) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = mcRow[p], k0 = rp[i], len = rp[i + 1] - k0;
+  for (int k = 0; k < W; ++k) mcCol[(size_t)k * n + p] = k < len ? col[k0 + k] : -1;
+}
+
+__global__ void k_mc_values(int n, int W, const int* __restrict__ mcRow, const int* __restrict__ rp,
+                            const double* __restrict__ ac, const double* __restrict__ anb, double* mcAc,
+                            double* mcAnb) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = mcRow[p], k0 = rp[i], len = rp[i + 1] - k0;
+  mcAc[p] = ac[i];
+  for (int k = 0; k < W; ++k) mcAnb[(size_t)k * n + p] = k < len ? anb[k0 + k] : 0.0;
+}
+
+__global__ void k_mc_bc(int n, const int* __restrict__ mcRow, const double* __restrict__ bc, double* mcBc) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) mcBc[p] = bc[mcRow[p]];
+}
+
+// One colour's rows. The colour kernels of a sweep follow one another as programmatic
+// dependent launches: a kernel starts while the previous colour is still running, loads what
+// does not depend on x (its rows' positions, bc, ac and the first kMcPre entries, all
+// coalesced), and only then waits (griddepcontrol.wait returns once the previous kernel has
+// completed and its writes are visible) before it gathers the neighbour values.
+constexpr int kMcPre = 4;
+
+__global__ void __launch_bounds__(kBlock) k_mc_rows(int cnt, int p0, int n, int W, const int* __restrict__ mcRow,
+                                                   const int* __restrict__ mcCol, const double* __restrict__ mcAnb,
+                                                   const double* __restrict__ mcAc,
+                                                   const double* __restrict__ mcBc, double* x) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cnt) return;
-  const int i = rows[t];
-  double v = bc[i];
-  for (int k = rp[i]; k < rp[i + 1]; ++k) v = v - anb[k] * x[col[k]];
-  x[i] = v / ac[i];
+  const int p = p0 + t;
+  const int i = mcRow[p];
+  const double b = mcBc[p], a = mcAc[p];
+  int j[kMcPre];
+  double w[kMcPre];
+#pragma unroll
+  for (int k = 0; k < kMcPre; ++k) {
+    j[k] = k < W ? mcCol[(size_t)k * n + p] : -1;
+    w[k] = k < W ? mcAnb[(size_t)k * n + p] : 0.0;
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  double xv[kMcPre];
+#pragma unroll
+  for (int k = 0; k < kMcPre; ++k) xv[k] = j[k] >= 0 ? x[j[k]] : 0.0;
+  double v = b;
+  bool end = false;
+#pragma unroll
+  for (int k = 0; k < kMcPre; ++k) {
+    end |= j[k] < 0;
+    if (!end) v = v - w[k] * xv[k];
+  }
+  if (!end) {
+    for (int k = kMcPre; k < W; ++k) {
+      const int jj = mcCol[(size_t)k * n + p];
+      if (jj < 0) break;
+      v = v - mcAnb[(size_t)k * n + p] * x[jj];
+    }
+  }
+  x[i] = v / a;
+}
+
+static int build_mc_pattern(LinCtx& c, Level& L) {
+  if (L.mc_valid) return UFVM_OK;
+  UFVM_CHECK(build_coloring(c, L));
+  const int n = L.n;
+  UFVM_CHECK(dalloc(L.mcRow, n));
+  DArr<int> flag, pos;
+  UFVM_CHECK(dalloc(flag, n));
+  UFVM_CHECK(dalloc(pos, n + 1));
+  for (int q = 0; q < L.ncolor; ++q) {
+    k_color_flag<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.color.p, q, flag.p);
+    UFVM_CHECK(scan_exclusive(c, flag.p, pos.p, n, nullptr));
+    k_color_place<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.color.p, q, L.h_colorStart[q], pos.p, L.mcRow.p);
+  }
+  UFVM_LAUNCH_CHECK();
+  UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 4, 0, sizeof(int), c.stream));
+  k_row_len_max<<<nblocks(n), kBlock, 0, c.stream>>>(n, L.rowptr.p, c.iflag.p + 4);
+  UFVM_LAUNCH_CHECK();
+  int W = 0;
+  UFVM_CUDA(cudaMemcpyAsync(&W, c.iflag.p + 4, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  UFVM_CUDA(cudaStreamSynchronize(c.stream));
+  L.mcW = W;
+  const size_t cap = std::max<size_t>((size_t)W * n, 1);
+  UFVM_CHECK(dalloc(L.mcCol, cap));
+  UFVM_CHECK(dalloc(L.mcAnb, cap));
+  UFVM_CHECK(dalloc(L.mcAc, n));
+  UFVM_CHECK(dalloc(L.mcBc, n));
+  k_mc_pattern<<<nblocks(n), kBlock, 0, c.stream>>>(n, W, L.mcRow.p, L.rowptr.p, L.col.p, L.mcCol.p);
+  UFVM_LAUNCH_CHECK();
+  dfree(flag);
+  dfree(pos);
+  L.mc_valid = true;
+  L.mc_epoch = 0;
+  return UFVM_OK;
+}
+
+// Copies the matrix (once per AMG solve, or on every call outside one) and the right-hand
+// side (every call) into the colour-major layout.
+int mcgs_prepare(LinCtx& c, Level& L) {
+  UFVM_CHECK(c.ensure(L.n));
+  UFVM_CHECK(build_mc_pattern(c, L));
+  if (c.factor_epoch == 0 || L.mc_epoch != c.factor_epoch) {
+    k_mc_values<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.mcW, L.mcRow.p, L.rowptr.p, L.ac.p, L.anb.p, L.mcAc.p,
+                                                       L.mcAnb.p);
+    L.mc_epoch = c.factor_epoch;
+  }
+  k_mc_bc<<<nblocks(L.n), kBlock, 0, c.stream>>>(L.n, L.mcRow.p, L.bc.p, L.mcBc.p);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
 }
 
 int mcgs_sweep(LinCtx& c, Level& L) {
-  UFVM_CHECK(build_coloring(c, L));
+  if (!L.mc_valid) { set_error("mcgs_sweep: layout not prepared"); return UFVM_E_INVALID; }
+  // the first colour kernel of the sweep waits for all earlier work the ordinary way; the
+  // later ones are programmatic dependents of the colour before them
+  int launched = 0;
   for (int pass = 0; pass < 2; ++pass) {
     for (int q = 0; q < L.ncolor; ++q) {
       const int col_ = pass == 0 ? q : L.ncolor - 1 - q;
       const int s = L.h_colorStart[col_], cnt = L.h_colorStart[col_ + 1] - s;
       if (cnt <= 0) continue;
-      k_gs_rows<<<nblocks(cnt), kBlock, 0, c.stream>>>(cnt, L.colorRows.p + s, L.rowptr.p, L.col.p, L.ac.p, L.anb.p,
-                                                      L.bc.p, L.dphi.p);
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(nblocks(cnt));
+      cfg.blockDim = dim3(kBlock);
+      cfg.stream = c.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = launched > 0 ? 1 : 0;
+      UFVM_CUDA(cudaLaunchKernelEx(&cfg, k_mc_rows, cnt, s, L.n, L.mcW, (const int*)L.mcRow.p,
+                                   (const int*)L.mcCol.p, (const double*)L.mcAnb.p, (const double*)L.mcAc.p,
+                                   (const double*)L.mcBc.p, L.dphi.p));
+      ++launched;
     }
   }
-  UFVM_LAUNCH_CHECK();
   return UFVM_OK;
 }
 
@@ -703,6 +831,7 @@ int solve_algebraic_system(LinCtx& c, Level& L, int smoother, int n_iter, double
       ++it;
     }
   } else {
+    if (smoother != UFVM_SMOOTHER_SOR) UFVM_CHECK(mcgs_prepare(c, L));
     while (it <= n_iter && r1 > rrf * r0) {
       if (smoother == UFVM_SMOOTHER_SOR) UFVM_CHECK(gs_sweep(c, L));
       else UFVM_CHECK(mcgs_sweep(c, L));

@@ -10,8 +10,10 @@ int sum_abs_residual(LinCtx& c, const Level& L, const double* x, double* out_hos
 int build_schedule(LinCtx& c, Level& L);
 int build_tpos(LinCtx& c, Level& L);
 int build_coloring(LinCtx& c, Level& L);
+int check_barrier(LinCtx& c);                        // error if a grid-barrier sweep timed out
 int gs_sweep(LinCtx& c, Level& L);                   // natural-order symmetric GS (level scheduled)
-int mcgs_sweep(LinCtx& c, Level& L);                 // multicolour symmetric GS
+int mcgs_prepare(LinCtx& c, Level& L);               // colour-major copy of the matrix and rhs
+int mcgs_sweep(LinCtx& c, Level& L);                 // multicolour symmetric GS (after mcgs_prepare)
 int ilu_factor(LinCtx& c, Level& L, int quirks);     // dc = DILU diagonal inverse
 int ilu_sweep(LinCtx& c, Level& L);                  // one cfdSolveILU application
 int solve_algebraic_system(LinCtx& c, Level& L, int smoother, int n_iter, double rrf, int quirks,

@@ -106,6 +106,7 @@ def lib():
     L.ufvm_solve_algebraic_system.argtypes = [ct.c_int32, VP, VP, VP, VP, VP, VP, ct.c_int32, ct.c_int32,
                                               ct.c_double, ct.c_int32, D, D, I32, VP]
     L.ufvm_agglomerate_level.argtypes = [ct.c_int32, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, I32, VP]
+    L.ufvm_profile_plain_kernel.argtypes = [ct.c_int32, ct.c_int32, VP, VP, VP, VP, VP, VP, ct.c_int32, D, D, VP]
     _lib = L
     return L
 
@@ -337,6 +338,21 @@ def cfdSolveAlgebraicSystem(rowptr, col, ac, anb, bc, dphi, smoother: str = "ILU
                                              ct.byref(r1), ct.byref(it), _stream()))
     torch.cuda.synchronize()
     return x.cpu().numpy(), r0.value, r1.value, it.value
+
+
+PLAIN_KERNELS = {"residual": 0, "SOR": 1, "MCGS": 2, "ILU": 3}
+
+
+def profile_plain_kernel(kernel: str, rowptr, col, ac, anb, bc, dphi, reps: int = 5):
+    """Kernel time of one stand-alone solver kernel on DEVICE tensors (the plain form's roofline
+    measurement): "residual", "SOR" (level-scheduled natural-order sweep), "MCGS" (multicolour
+    sweep) or "ILU" (one DILU application). L2 is flushed (by reads) before every timed launch.
+    Returns (ms per launch, algorithmic bytes per launch). Sweeps overwrite dphi."""
+    ms, by = ct.c_double(), ct.c_double()
+    _check(lib().ufvm_profile_plain_kernel(PLAIN_KERNELS[kernel], len(ac), _ptr(rowptr), _ptr(col), _ptr(ac),
+                                           _ptr(anb), _ptr(bc), _ptr(dphi), int(reps), ct.byref(ms), ct.byref(by),
+                                           _stream()))
+    return ms.value, by.value
 
 
 def cfdAgglomerateLevel(rowptr, col, ac, anb):

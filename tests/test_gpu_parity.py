@@ -69,13 +69,44 @@ def test_residual_sor_ilu_bit_exact(ufvm_mod, oracle_mod, which):
         same(dc, oracle_mod.ilu_factor(rp, col, ac, anb, q), "ILU factor")
     same(ufvm_mod.cfdSolveILU(rp, col, ac, anb, bc, dc, x0), oracle_mod.ilu_sweep(rp, col, ac, anb, bc, dc, x0),
          "ILU solve")
-    for sm in ("ILU", "SOR"):
+    for sm in ("ILU", "SOR", "MCGS"):
         xg, r0g, r1g, itg = ufvm_mod.cfdSolveAlgebraicSystem(rp, col, ac, anb, bc, x0, sm, 10, 0.1)
         xo, r0o, r1o, ito = oracle_mod.solve_algebraic_system(rp, col, ac, anb, bc, x0, case.SMOOTHER[sm], 10, 0.1,
                                                               case.QUIRKS_REFERENCE)
         assert itg == ito, sm
         same(xg, xo, "cfdSolveAlgebraicSystem " + sm)
         assert abs(r0g - r0o) <= RTOL_NORM * abs(r0o) and abs(r1g - r1o) <= RTOL_NORM * abs(r1o)
+
+
+@pytest.mark.parametrize("which", ["random", "cavity"])
+def test_profiled_kernels_do_the_work(ufvm_mod, oracle_mod, which):
+    """The kernel-timing entry point times the real sweeps: after it, dphi equals 1 + reps
+    sweeps of the oracle (one untimed launch, then reps timed ones), bit for bit."""
+    import torch
+    if which == "random":
+        rp, col, ac, anb, bc = random_diag_dominant(3000, 5, nbr=6)
+    else:
+        rp, col, ac, anb, bc = _p_system(oracle_mod, case.cavity_case(24, nu=0.01))
+    x0 = np.random.default_rng(3).normal(size=len(ac)) * 1e-3
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (rp, col, ac, anb, bc)]
+    reps = 2
+    nc, color = oracle_mod.coloring(rp, col)
+    dc = oracle_mod.ilu_factor(rp, col, ac, anb, 0)
+    step = {"SOR": lambda x: oracle_mod.sor_sweep(rp, col, ac, anb, bc, x),
+            "MCGS": lambda x: oracle_mod.mcgs_sweep(rp, col, ac, anb, bc, color, nc, x),
+            "ILU": lambda x: oracle_mod.ilu_sweep(rp, col, ac, anb, bc, dc, x)}
+    for name, f in step.items():
+        x = torch.from_numpy(x0.copy()).cuda()
+        ms, by = ufvm_mod.profile_plain_kernel(name, *dev, x, reps)
+        assert ms > 0 and by > 0
+        want = x0.copy()
+        for _ in range(1 + reps):
+            want = f(want)
+        same(x.cpu().numpy(), want, "profiled " + name)
+    x = torch.from_numpy(x0.copy()).cuda()
+    ms, by = ufvm_mod.profile_plain_kernel("residual", *dev, x, reps)
+    assert ms > 0 and by == 36.0 * len(ac) + 12.0 * len(col)
+    same(x.cpu().numpy(), x0, "residual leaves dphi")
 
 
 @pytest.mark.parametrize("which", ["random", "cavity20", "cavity64", "channel"])
@@ -134,9 +165,13 @@ def test_stage_by_stage_bit_exact(ufvm_mod, oracle_mod, name):
             _compare_case(g, oc, ("U", "p", "PP", "gradPP", "mdot"))
 
 
-@pytest.mark.parametrize("name,iters", [("cavity20", 10), ("channel_small", 4), ("cylinder", 5)])
+@pytest.mark.parametrize("name,iters", [("cavity20", 10), ("channel_small", 4), ("cylinder", 5),
+                                        ("cavity20_mcgs", 6)])
 def test_iterations_bit_exact(ufvm_mod, oracle_mod, name, iters):
-    spec = SPECS[name]()
+    if name == "cavity20_mcgs":  # the multicolour smoother for U and p inside the AMG
+        spec = case.CaseSpec(**{**case.cavity_case(20, nu=0.01).__dict__, "p_smoother": "MCGS", "u_smoother": "MCGS"})
+    else:
+        spec = SPECS[name]()
     g = ufvm_mod.GpuCase(spec)
     oc = oracle_mod.OracleCase(spec)
     for it in range(iters):
