@@ -39,3 +39,18 @@ def test_no_cpu_fallback_without_gpu(ufvm_mod):
     from matlab_ufvm_b200 import case
     with pytest.raises(ufvm_mod.UfvmError):
         ufvm_mod.GpuCase(case.cavity_case(4))
+
+
+def test_profile_entry_rejects_bad_arguments(ufvm_mod):
+    """The kernel-timing entry point validates its arguments before any device work."""
+    lib = ufvm_mod.lib()
+    ms, by = ctypes.c_double(), ctypes.c_double()
+    P = ctypes.c_void_p
+    fake = P(16)  # never dereferenced: every call below is rejected first
+    for kernel, n, reps, ptr in ((4, 10, 1, fake), (-1, 10, 1, fake), (0, 0, 1, fake), (0, 10, 0, fake),
+                                 (0, 10, 1, P(None))):
+        st = lib.ufvm_profile_plain_kernel(kernel, n, ptr, ptr, ptr, ptr, ptr, ptr, reps, ctypes.byref(ms),
+                                           ctypes.byref(by), P(None))
+        assert st == 1, (kernel, n, reps, st)  # UFVM_E_INVALID
+    assert b"bad argument" in lib.ufvm_last_error()
+    assert set(ufvm_mod.PLAIN_KERNELS) == {"residual", "SOR", "MCGS", "ILU"}
