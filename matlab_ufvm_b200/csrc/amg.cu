@@ -411,6 +411,11 @@ void free_level(Level& L, bool keep_matrix) {
   dfree(L.perm); dfree(L.inv); dfree(L.ellCol); dfree(L.parentsP); dfree(L.childP); dfree(L.childStartP); dfree(L.gpos);
   dfree(L.ellAnb); dfree(L.uAnb); dfree(L.uAc); dfree(L.uBc); dfree(L.uX);
   dfree(L.mcRow); dfree(L.mcCol); dfree(L.mcAnb); dfree(L.mcAc); dfree(L.mcBc);
+  for (int k = 0; k < 4; ++k) {
+    dfree(L.sellCol[k]); dfree(L.sellA[k]);
+    L.sell_valid[k] = false;
+    L.sell_epoch[k] = 0;
+  }
   L.mc_valid = false;
   L.mc_epoch = 0;
   L.ell_valid = false;

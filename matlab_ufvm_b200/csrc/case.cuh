@@ -41,6 +41,16 @@ struct Level {
   // dc holds the DILU factor of the current matrix while dc_epoch equals the solver's epoch
   unsigned long long dc_epoch = 0;
   int dc_quirks = 0;
+  // Position-ordered ELL copies for the narrow level-scheduled sweeps, one per kind (0: GS
+  // forward, all entries; 1: GS backward, all entries; 2: DILU forward, lower entries by
+  // increasing column; 3: DILU backward, upper entries): entry t of schedule position p at
+  // [t * n + p] (column -1 past the row's end), coefficients copied from the matrix;
+  // sell_epoch as dc_epoch for the copied coefficients
+  bool sell_valid[4] = {false, false, false, false};
+  int sellW[4] = {0, 0, 0, 0};
+  unsigned long long sell_epoch[4] = {0, 0, 0, 0};
+  DArr<int> sellCol[4];
+  DArr<double> sellA[4];
   // multicolour ordering
   bool color_valid = false;
   int ncolor = 0;

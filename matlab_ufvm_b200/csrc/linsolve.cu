@@ -296,6 +296,7 @@ int build_schedule(LinCtx& c, Level& L) {
   UFVM_LAUNCH_CHECK();
   L.sched_valid = true;
   L.dc_epoch = 0;
+  for (int k = 0; k < 4; ++k) L.sell_valid[k] = false;
   return UFVM_OK;
 }
 
@@ -455,11 +456,306 @@ __global__ void k_ilu_res(int n, const int* __restrict__ rp, const int* __restri
   rc[i] = res;
 }
 
+// ---------------------------------------------------------------- position-ordered sweeps
+// The narrow sweeps read each row through a position-ordered ELL copy: schedule position p
+// (row i = rows[p]) keeps its entries at [t * n + p], so one coalesced load per array brings a
+// level's rows, and nothing but the neighbour values is left to load after the barrier. The
+// next level's rows are fetched between the barrier's arrive and its wait (cluster form) or
+// before it (single CTA). Each row performs the same operations on the same operands, in the
+// same order, as row_op: same bits.
+enum { SELL_GS_FWD = 0, SELL_GS_BWD = 1, SELL_ILU_FWD = 2, SELL_ILU_BWD = 3 };
+
+// Entries of row i for one kind, in the kind's order: callback(t, q) with q the CSR position.
+template <int KIND, typename F>
+__device__ __forceinline__ int sell_entries(int i, const int* __restrict__ rp, const int* __restrict__ col,
+                                            const int* __restrict__ lord, F f) {
+  const int k0 = rp[i], k1 = rp[i + 1];
+  int t = 0;
+  if (KIND == SELL_GS_FWD || KIND == SELL_GS_BWD) {
+    for (int k = k0; k < k1; ++k) f(t++, k);
+  } else if (KIND == SELL_ILU_FWD) {
+    for (int k = k0; k < k1; ++k) {
+      const int q = lord[k];
+      if (q < 0) break;
+      f(t++, q);
+    }
+  } else {
+    for (int k = k0; k < k1; ++k)
+      if (col[k] > i) f(t++, k);
+  }
+  return t;
+}
+
+template <int KIND>
+__global__ void k_sell_width(int n, const int* __restrict__ rows, const int* __restrict__ rp,
+                             const int* __restrict__ col, const int* __restrict__ lord, int* wmax) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int w = sell_entries<KIND>(rows[p], rp, col, lord, [](int, int) {});
+  atomicMax(wmax, w);
+}
+
+// VALUES = false: columns (-1 past the end); true: coefficients.
+template <int KIND, bool VALUES>
+__global__ void k_sell_fill(int n, int W, const int* __restrict__ rows, const int* __restrict__ rp,
+                            const int* __restrict__ col, const int* __restrict__ lord,
+                            const double* __restrict__ anb, int* scol, double* sa) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = rows[p];
+  const int cnt = sell_entries<KIND>(i, rp, col, lord, [&](int t, int q) {
+    if (VALUES) sa[(size_t)t * n + p] = anb[q];
+    else scol[(size_t)t * n + p] = col[q];
+  });
+  for (int t = cnt; t < W; ++t) {
+    if (VALUES) sa[(size_t)t * n + p] = 0.0;
+    else scol[(size_t)t * n + p] = -1;
+  }
+}
+
+struct SellArgs {
+  int n, nlev, W;
+  const int *lstart, *rows, *scol;
+  const double *sa, *ac, *bc, *dc;
+  double *x, *rc;
+};
+
+constexpr int kSellPre = 4;
+
+// What a row needs that no other row of the sweep writes: its own values and its first
+// kSellPre entries.
+struct SellRow {
+  int i;
+  double own0, own1, own2;
+  int c[kSellPre];
+  double w[kSellPre];
+};
+
+template <int OP>
+__device__ __forceinline__ void sell_load(SellRow& r, const SellArgs& a, int p) {
+  r.i = -1;
+  if (p < 0) return;
+  const int i = a.rows[p];
+  r.i = i;
+  if (OP == OP_GS) {
+    r.own0 = a.bc[i];
+    r.own1 = a.ac[i];
+  } else if (OP == OP_ILU_FWD) {
+    r.own0 = __ldcg(a.rc + i);
+  } else {  // OP_ILU_BWD
+    r.own0 = __ldcg(a.rc + i);
+    r.own1 = a.dc[i];
+    r.own2 = a.x[i];
+  }
+#pragma unroll
+  for (int t = 0; t < kSellPre; ++t) {
+    const bool in = t < a.W;
+    r.c[t] = in ? a.scol[(size_t)t * a.n + p] : -1;
+    r.w[t] = in ? a.sa[(size_t)t * a.n + p] : 0.0;
+  }
+}
+
+template <int OP>
+__device__ __forceinline__ void sell_finish(const SellRow& r, const SellArgs& a, int p) {
+  const int i = r.i;
+  // neighbour values (and, for the DILU forward substitution, the factor of the neighbour)
+  double g[kSellPre], h[kSellPre];
+#pragma unroll
+  for (int t = 0; t < kSellPre; ++t) {
+    const bool in = r.c[t] >= 0;
+    g[t] = in ? (OP == OP_GS ? __ldcg(a.x + r.c[t]) : __ldcg(a.rc + r.c[t])) : 0.0;
+    if (OP == OP_ILU_FWD) h[t] = in ? a.dc[r.c[t]] : 0.0;
+  }
+  double v = r.own0;
+  bool end = false;
+  if (OP == OP_ILU_BWD && i >= a.n - 1) end = true;  // the reference skips the last row's sum
+#pragma unroll
+  for (int t = 0; t < kSellPre; ++t) {
+    end |= r.c[t] < 0;
+    if (!end) {
+      if (OP == OP_ILU_FWD) {
+        const double mat1 = h[t] * g[t];
+        v = v - r.w[t] * mat1;
+      } else {
+        v = v - r.w[t] * g[t];
+      }
+    }
+  }
+  if (!end) {
+    for (int t = kSellPre; t < a.W; ++t) {
+      const int j = a.scol[(size_t)t * a.n + p];
+      if (j < 0) break;
+      const double wt = a.sa[(size_t)t * a.n + p];
+      if (OP == OP_ILU_FWD) {
+        const double mat1 = a.dc[j] * __ldcg(a.rc + j);
+        v = v - wt * mat1;
+      } else if (OP == OP_GS) {
+        v = v - wt * __ldcg(a.x + j);
+      } else {
+        v = v - wt * __ldcg(a.rc + j);
+      }
+    }
+  }
+  if (OP == OP_GS) {
+    __stcg(a.x + i, v / r.own1);
+  } else if (OP == OP_ILU_FWD) {
+    __stcg(a.rc + i, v);
+  } else {
+    const double mat1 = r.own1 * v;
+    __stcg(a.rc + i, mat1);
+    a.x[i] = r.own2 + mat1;
+  }
+}
+
+template <int OP, bool CLUSTER>
+__global__ void __launch_bounds__(1024) k_sched_sell(SellArgs a) {
+  unsigned int rank = 0, size = 1;
+  if (CLUSTER) {
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(size));
+  }
+  const int tid = (int)rank * blockDim.x + threadIdx.x, nth = (int)size * blockDim.x;
+  SellRow pre;
+  {
+    const int e = a.lstart[1];
+    sell_load<OP>(pre, a, tid < e ? tid : -1);
+  }
+  for (int L = 0; L < a.nlev; ++L) {
+    const int s = a.lstart[L], e = a.lstart[L + 1];
+    if (s + tid < e) sell_finish<OP>(pre, a, s + tid);
+    for (int p = s + tid + nth; p < e; p += nth) {
+      SellRow r;
+      sell_load<OP>(r, a, p);
+      sell_finish<OP>(r, a, p);
+    }
+    if (L + 1 < a.nlev) {
+      const int s2 = a.lstart[L + 1], e2 = a.lstart[L + 2];
+      if (CLUSTER) {
+        asm volatile("barrier.cluster.arrive.release;\n" ::: "memory");
+        sell_load<OP>(pre, a, s2 + tid < e2 ? s2 + tid : -1);
+        asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
+      } else {
+        sell_load<OP>(pre, a, s2 + tid < e2 ? s2 + tid : -1);
+        __syncthreads();
+      }
+    }
+  }
+}
+
+template <int KIND>
+static int sell_prepare_kind(LinCtx& c, Level& L) {
+  const int n = L.n;
+  const int* rows = (KIND == SELL_GS_FWD || KIND == SELL_ILU_FWD) ? L.fwdRows.p : L.bwdRows.p;
+  if (!L.sell_valid[KIND]) {
+    UFVM_CUDA(cudaMemsetAsync(c.iflag.p + 5, 0, sizeof(int), c.stream));
+    k_sell_width<KIND><<<nblocks(n), kBlock, 0, c.stream>>>(n, rows, L.rowptr.p, L.col.p, L.lord.p, c.iflag.p + 5);
+    UFVM_LAUNCH_CHECK();
+    int W = 0;
+    UFVM_CUDA(cudaMemcpyAsync(&W, c.iflag.p + 5, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    UFVM_CUDA(cudaStreamSynchronize(c.stream));
+    const size_t cap = std::max<size_t>((size_t)W * n, 1);
+    UFVM_CHECK(dalloc(L.sellCol[KIND], cap));
+    UFVM_CHECK(dalloc(L.sellA[KIND], cap));
+    L.sellW[KIND] = W;
+    k_sell_fill<KIND, false><<<nblocks(n), kBlock, 0, c.stream>>>(n, W, rows, L.rowptr.p, L.col.p, L.lord.p, nullptr,
+                                                                 L.sellCol[KIND].p, nullptr);
+    UFVM_LAUNCH_CHECK();
+    L.sell_valid[KIND] = true;
+    L.sell_epoch[KIND] = 0;
+  }
+  // the copied coefficients follow the matrix: once per AMG solve, on every call outside one
+  if (c.factor_epoch == 0 || L.sell_epoch[KIND] != c.factor_epoch) {
+    k_sell_fill<KIND, true><<<nblocks(n), kBlock, 0, c.stream>>>(n, L.sellW[KIND], rows, L.rowptr.p, L.col.p,
+                                                                L.lord.p, L.anb.p, nullptr, L.sellA[KIND].p);
+    UFVM_LAUNCH_CHECK();
+    L.sell_epoch[KIND] = c.factor_epoch;
+  }
+  return UFVM_OK;
+}
+
 // Rows a cluster sweep handles per thread and level before the wide (grid) form pays off.
 constexpr int kClusterRowsPerThread = 4;
 
+// 0: the wide grid form; 1: one CTA; 2, 4 or 8: one cluster of that many 1024-thread CTAs.
+template <int OP>
+static int sweep_shape(LinCtx& c, const Level& L) {
+  const int w = std::max(L.maxw, 1);
+  if (w <= 1024) return 1;
+  if (w > 8 * 1024 * kClusterRowsPerThread) return 0;
+  if (c.cluster_ok == 0) {
+    // once per context: can a cluster of 8 such CTAs be resident?
+    cudaLaunchConfig_t q = {};
+    q.gridDim = dim3(8);
+    q.blockDim = dim3(1024);
+    q.stream = c.stream;
+    cudaLaunchAttribute qa[1];
+    qa[0].id = cudaLaunchAttributeClusterDimension;
+    qa[0].val.clusterDim.x = 8;
+    qa[0].val.clusterDim.y = 1;
+    qa[0].val.clusterDim.z = 1;
+    q.attrs = qa;
+    q.numAttrs = 1;
+    int ncl = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveClusters(&ncl, (const void*)k_sched_sell<OP_ILU_FWD, true>, &q);
+    int ncl2 = 0;
+    const cudaError_t e2 = cudaOccupancyMaxActiveClusters(&ncl2, (const void*)k_sched_sweep_cl<OP_ILU_FACT, true>, &q);
+    if (e != cudaSuccess || e2 != cudaSuccess) (void)cudaGetLastError();
+    c.cluster_ok = (e == cudaSuccess && e2 == cudaSuccess && ncl >= 1 && ncl2 >= 1) ? 1 : -1;
+  }
+  if (c.cluster_ok < 0) return 0;
+  int cs = 2;
+  while (cs < 8 && cs * 1024 < w) cs *= 2;
+  return cs;
+}
+
+template <typename K, typename A>
+static int launch_cluster(K kernel, int cs, cudaStream_t st, const A& args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(1024);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  UFVM_CUDA(cudaLaunchKernelEx(&cfg, kernel, args));
+  return UFVM_OK;
+}
+
 template <int OP>
 static int launch_sweep(LinCtx& c, Level& L, bool fwd, int quirks) {
+  const int shape = sweep_shape<OP>(c, L);
+  const int w = std::max(L.maxw, 1);
+  const int bs1 = std::min(1024, std::max(32, (w + 31) / 32 * 32));
+  if (shape != 0 && OP != OP_ILU_FACT) {
+    constexpr int kind = OP == OP_GS ? -1 : (OP == OP_ILU_FWD ? SELL_ILU_FWD : SELL_ILU_BWD);
+    const int k = kind >= 0 ? kind : (fwd ? SELL_GS_FWD : SELL_GS_BWD);
+    switch (k) {
+      case SELL_GS_FWD: UFVM_CHECK(sell_prepare_kind<SELL_GS_FWD>(c, L)); break;
+      case SELL_GS_BWD: UFVM_CHECK(sell_prepare_kind<SELL_GS_BWD>(c, L)); break;
+      case SELL_ILU_FWD: UFVM_CHECK(sell_prepare_kind<SELL_ILU_FWD>(c, L)); break;
+      default: UFVM_CHECK(sell_prepare_kind<SELL_ILU_BWD>(c, L)); break;
+    }
+    SellArgs s;
+    s.n = L.n;
+    s.nlev = fwd ? L.nfwd : L.nbwd;
+    s.W = L.sellW[k];
+    s.lstart = fwd ? L.fwdStart.p : L.bwdStart.p;
+    s.rows = fwd ? L.fwdRows.p : L.bwdRows.p;
+    s.scol = L.sellCol[k].p;
+    s.sa = L.sellA[k].p;
+    s.ac = L.ac.p; s.bc = L.bc.p; s.dc = L.dc.p;
+    s.x = L.dphi.p; s.rc = L.rc.p;
+    if (shape == 1) {
+      k_sched_sell<OP, false><<<1, bs1, 0, c.stream>>>(s);
+      UFVM_LAUNCH_CHECK();
+      return UFVM_OK;
+    }
+    return launch_cluster(k_sched_sell<OP, true>, shape, c.stream, s);
+  }
   SweepArgs a;
   a.n = L.n; a.quirks = quirks;
   a.nlev = fwd ? L.nfwd : L.nbwd;
@@ -468,45 +764,12 @@ static int launch_sweep(LinCtx& c, Level& L, bool fwd, int quirks) {
   a.rp = L.rowptr.p; a.col = L.col.p; a.tpos = L.tpos.p; a.lord = L.lord.p;
   a.ac = L.ac.p; a.anb = L.anb.p; a.bc = L.bc.p;
   a.x = L.dphi.p; a.dc = L.dc.p; a.rc = L.rc.p;
-  const int w = std::max(L.maxw, 1);
-  if (w <= 1024) {
-    const int bs = std::min(1024, std::max(32, (w + 31) / 32 * 32));
-    k_sched_sweep_cl<OP, false><<<1, bs, 0, c.stream>>>(a);
+  if (shape == 1) {
+    k_sched_sweep_cl<OP, false><<<1, bs1, 0, c.stream>>>(a);
     UFVM_LAUNCH_CHECK();
     return UFVM_OK;
   }
-  if (w <= 8 * 1024 * kClusterRowsPerThread && c.cluster_ok >= 0) {
-    int cs = 2;
-    while (cs < 8 && cs * 1024 < w) cs *= 2;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = c.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cs;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (c.cluster_ok == 0) {
-      // once per context: can a cluster of 8 such CTAs be resident?
-      int ncl = 0;
-      cudaLaunchConfig_t q = cfg;
-      q.gridDim = dim3(8);
-      cudaLaunchAttribute qa[1] = {attr[0]};
-      qa[0].val.clusterDim.x = 8;
-      q.attrs = qa;
-      const cudaError_t e = cudaOccupancyMaxActiveClusters(&ncl, (const void*)k_sched_sweep_cl<OP, true>, &q);
-      if (e != cudaSuccess) (void)cudaGetLastError();
-      c.cluster_ok = (e == cudaSuccess && ncl >= 1) ? 1 : -1;
-    }
-    if (c.cluster_ok > 0) {
-      UFVM_CUDA(cudaLaunchKernelEx(&cfg, k_sched_sweep_cl<OP, true>, a));
-      return UFVM_OK;
-    }
-  }
+  if (shape > 1) return launch_cluster(k_sched_sweep_cl<OP, true>, shape, c.stream, a);
   GridBarrier gb{c.bar.p, c.bar.p + 1, c.berr.p};
   int maxb = 0;
   UFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxb, k_sched_sweep<OP>, kBlock, 0));
