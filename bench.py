@@ -505,9 +505,9 @@ def plain_kernel_rooflines(peaks):
     for key, name in (
             ("residual", "k_residual (plain FP64 r = b - A x, cfdComputeResidualsArray)"),
             ("MCGS", "k_mc_rows (plain FP64 symmetric multicolour Gauss-Seidel, colour-major ELL copy)"),
-            ("SOR", "k_sched_sweep_cl (plain FP64 symmetric natural-order Gauss-Seidel, level scheduled, "
+            ("SOR", "k_sched_sell (plain FP64 symmetric natural-order Gauss-Seidel, level scheduled, "
                     "cfdSolveSOR: latency-bound by its dependency levels)"),
-            ("ILU", "k_ilu_res + k_sched_sweep_cl (plain FP64 DILU application, level scheduled, cfdSolveILU: "
+            ("ILU", "k_ilu_res + k_sched_sell (plain FP64 DILU application, level scheduled, cfdSolveILU: "
                     "latency-bound by its dependency levels)")):
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
         ms, by = ufvm.profile_plain_kernel(key, *dev, x, 5)
