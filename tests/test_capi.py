@@ -54,3 +54,54 @@ def test_profile_entry_rejects_bad_arguments(ufvm_mod):
         assert st == 1, (kernel, n, reps, st)  # UFVM_E_INVALID
     assert b"bad argument" in lib.ufvm_last_error()
     assert set(ufvm_mod.PLAIN_KERNELS) == {"residual", "SOR", "MCGS", "ILU"}
+
+
+def _header_struct_fields(name):
+    """(field, C type) pairs of a `typedef struct { ... } name;` in include/ufvm.h."""
+    txt = open(os.path.join(ROOT, "include", "ufvm.h")).read()
+    txt = re.sub(r"/\*.*?\*/", " ", txt, flags=re.S)
+    body = re.search(r"typedef struct\s*\{([^}]*)\}\s*" + name + r"\s*;", txt).group(1)
+    out = []
+    for decl in body.split(";"):
+        decl = " ".join(decl.split())
+        if not decl:
+            continue
+        m = re.match(r"((?:const )?[a-z0-9_]+\s*\*?)\s*(.*)", decl)
+        ctype, names = m.group(1).replace(" ", ""), m.group(2)
+        for nm in names.split(","):
+            nm = nm.strip()
+            star = nm.startswith("*")
+            out.append((nm.lstrip("*").strip(), ctype + ("*" if star else "")))
+    return out
+
+
+@pytest.mark.parametrize("cname,pyname", [("ufvm_mesh_desc", "MeshDesc"), ("ufvm_settings", "Settings")])
+def test_ctypes_structs_match_header_layout(ufvm_mod, cname, pyname, tmp_path):
+    """The Python mirror's ctypes structs have the header's fields, in order, at the offsets
+    the C compiler gives them (a drift here would hand the library shifted settings)."""
+    import shutil
+    import subprocess
+    fields = _header_struct_fields(cname)
+    py = getattr(ufvm_mod, pyname)
+    assert [f[0] for f in py._fields_] == [f[0] for f in fields]
+    for (nm, ctype), (pnm, ptype) in zip(fields, py._fields_):
+        if ctype.endswith("*"):
+            assert issubclass(ptype, (ctypes._Pointer, ctypes.c_void_p)), nm
+        else:
+            assert ptype is {"int32_t": ctypes.c_int32, "double": ctypes.c_double}[ctype], nm
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ufvm.h"', "int main(void) {",
+             f'  printf("size %zu\\n", sizeof({cname}));']
+    lines += [f'  printf("{nm} %zu\\n", offsetof({cname}, {nm}));' for nm, _ in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                       text=True).stdout.splitlines())
+    assert int(got["size"]) == ctypes.sizeof(py)
+    for nm, _ in fields:
+        assert int(got[nm]) == getattr(py, nm).offset, nm
