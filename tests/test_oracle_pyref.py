@@ -58,3 +58,43 @@ def test_coloring_is_proper_and_deterministic(oracle_mod):
     assert np.array_equal(c1, c2) and c1.min() >= 0 and c1.max() == nc - 1
     for i in range(len(rp) - 1):
         assert np.all(c1[col[rp[i]:rp[i + 1]]] != c1[i])
+
+
+def _py_greedy_colouring(rp, col):
+    """First-fit colouring in natural order: each row takes the smallest colour that none of
+    its lower-numbered neighbours has."""
+    n = len(rp) - 1
+    c = np.zeros(n, dtype=np.int64)
+    for i in range(n):
+        used = {int(c[j]) for j in col[rp[i]:rp[i + 1]] if j < i}
+        k = 0
+        while k in used:
+            k += 1
+        c[i] = k
+    return c
+
+
+def _py_mcgs(rp, col, ac, anb, bc, colour, x0):
+    """Symmetric multicolour Gauss-Seidel: colours ascending then descending, each row
+    v = bc - sum anb * x in cconn order, x = v / ac."""
+    x = np.array(x0, dtype=np.float64)
+    nc = int(colour.max()) + 1
+    for c in list(range(nc)) + list(range(nc - 1, -1, -1)):
+        for i in np.flatnonzero(colour == c):
+            v = bc[i]
+            for k in range(rp[i], rp[i + 1]):
+                v = v - anb[k] * x[col[k]]
+            x[i] = v / ac[i]
+    return x
+
+
+@pytest.mark.parametrize("seed", [0, 4])
+def test_mcgs_matches_transliteration(oracle_mod, seed):
+    """The oracle's multicolour smoother (the multicolour form of solve/cfdSolveSOR.m:13-29)
+    against the definition above: same colouring, same sweep, bit for bit."""
+    rp, col, ac, anb, bc = random_diag_dominant(200, seed, nbr=6)
+    nc, colour = oracle_mod.coloring(rp, col)
+    assert np.array_equal(colour, _py_greedy_colouring(rp, col))
+    x0 = np.random.default_rng(seed).normal(size=200)
+    assert np.array_equal(oracle_mod.mcgs_sweep(rp, col, ac, anb, bc, colour, nc, x0),
+                          _py_mcgs(rp, col, ac, anb, bc, colour, x0))
