@@ -62,6 +62,11 @@ def parse():
     ap.add_argument("--profile-plain", choices=("C1", "C2", "C3"), default=None,
                     help="profiling run for ncu: one plain FP64 SIMPLE iteration of a named single-case "
                          "workload inside cudaProfilerStart/Stop (after one warm-up iteration)")
+    ap.add_argument("--workload", choices=("sweep", "serving"), default="sweep",
+                    help="sweep: the 2D cavity sweep stream (the headline line); serving: the Poisson-arrival mix "
+                         "of 2D/3D cavities and tet channels (its own JSON line)")
+    ap.add_argument("--serving-requests", type=int, default=48, help="requests per serving phase")
+    ap.add_argument("--capacity-steps", type=int, default=400, help="service steps of the closed-loop phase")
     ap.add_argument("--plain-kernels", action="store_true",
                     help="only the plain FP64 form's solver-kernel rooflines on the 1M-cell tet channel (one JSON "
                          "line per kernel; the ncu target for those kernels)")
@@ -680,6 +685,62 @@ def main_ours(args):
     return 0
 
 
+def _serving_worker(key):
+    from matlab_ufvm_b200 import serving
+    kind, size = key
+    return key, serving.request_spec(serving.Request(0, kind, size, 100.0))
+
+
+def main_serving(args):
+    """The serving mix on one GPU: 70% 2D cavities of 1k-64k cells, 25% 3D cavities 32^3-96^3,
+    5% tet channels of 0.5-2M cells, Re 50..1000. A closed-loop phase (queue kept full) measures
+    the capacity in converged cases per second of service clock; an open-loop phase on a fresh
+    service then submits a second seeded stream at Poisson arrival times of 0.8 x that rate and
+    reports throughput and time-to-converge percentiles from arrival."""
+    import dataclasses
+    import multiprocessing as mp
+    import torch
+    from matlab_ufvm_b200 import build as _b, serving, ufvm
+    torch.cuda.set_device(0)
+    _b.build()
+    cap_reqs = serving.serving_mix(args.serving_requests, seed=101)
+    open_reqs = serving.serving_mix(args.serving_requests, seed=202)
+    keys = sorted({(r.kind, r.size) for r in cap_reqs + open_reqs}, key=lambda k: -serving.Request(0, *k, 1.0).cells)
+    base = {}
+    procs = max(1, min(len(keys), (os.cpu_count() or 2) - 1, 16))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        for key, spec in pool.imap_unordered(_serving_worker, keys):
+            base[key] = spec
+
+    def spec_fn(req):
+        return dataclasses.replace(base[(req.kind, req.size)], nu=1.0 / req.re, name=f"serving{req.index}")
+
+    settings = ufvm.fast_settings(base_spec(16))
+
+    def service():
+        svc = ufvm.Service(settings, max_resident_cells=args.budget)
+        svc.set_admit_interval(args.admit_interval)
+        return svc
+
+    svc = service()
+    cap = serving.closed_loop_capacity(svc, cap_reqs, args.capacity_steps, spec_fn=spec_fn)
+    svc.close()
+    rate = 0.8 * cap["cases_per_s"]
+    line = {"workload": "serving mix (70% 2D cavities 1k-64k cells, 25% 3D cavities 32^3-96^3, 5% tet channels "
+                        "0.5-2M cells, Re 50..1000, seeded)", "n_gpus": 1, "budget_cells": args.budget,
+            "capacity": cap, "arrival_rate_per_s": rate}
+    if rate > 0:
+        svc = service()
+        arr = serving.poisson_arrivals(len(open_reqs), rate, seed=303)
+        ol = serving.OpenLoop(svc, open_reqs, arr, spec_fn=spec_fn)
+        out = ol.run()
+        svc.close()
+        line.update(metric="converged cases/s + p50/p99 time to converge (from arrival, service clock)",
+                    open_loop=serving.summarize(out), service_steps=ol.steps, idle_s=ol.idle_s)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -688,6 +749,8 @@ def main():
         return main_profile(args)
     if args.profile_plain:
         return main_profile_plain(args)
+    if args.workload == "serving":
+        return main_serving(args)
     if args.plain_kernels:
         import torch
         from matlab_ufvm_b200 import build as _b
