@@ -156,10 +156,13 @@ int ufvm_case_sizes(const ufvm_case* c, int64_t* s) {
   return UFVM_OK;
 }
 
-int ufvm_update_fields(ufvm_case* c) { API_GUARD(c->c.update_fields()); }
+int ufvm_update_fields(ufvm_case* c) {
+  if (!c) return UFVM_E_INVALID;
+  API_GUARD(c->c.update_fields());
+}
 
 int ufvm_assemble_equation(ufvm_case* c, int eq, int comp, double* rms, double* mx) {
-  if (!c || !rms || !mx) return UFVM_E_INVALID;
+  if (!c || !rms || !mx || (eq != UFVM_EQ_U && eq != UFVM_EQ_P)) return UFVM_E_INVALID;
   if (eq == UFVM_EQ_U) {
     if (comp < 0 || comp > 2) return UFVM_E_INVALID;
     API_GUARD(c->c.assemble_u(comp, rms, mx));
@@ -168,13 +171,16 @@ int ufvm_assemble_equation(ufvm_case* c, int eq, int comp, double* rms, double* 
 }
 
 int ufvm_solve_equation(ufvm_case* c, int eq, double* r0, double* r1) {
-  if (!c || !r0 || !r1) return UFVM_E_INVALID;
+  if (!c || !r0 || !r1 || (eq != UFVM_EQ_U && eq != UFVM_EQ_P)) return UFVM_E_INVALID;
   API_GUARD(c->c.solve(eq, r0, r1));
 }
 
 int ufvm_correct_equation(ufvm_case* c, int eq, int comp) {
-  if (!c) return UFVM_E_INVALID;
-  if (eq == UFVM_EQ_U) API_GUARD(c->c.correct_u(comp));
+  if (!c || (eq != UFVM_EQ_U && eq != UFVM_EQ_P)) return UFVM_E_INVALID;
+  if (eq == UFVM_EQ_U) {
+    if (comp < 0 || comp > 2) return UFVM_E_INVALID;
+    API_GUARD(c->c.correct_u(comp));
+  }
   API_GUARD(c->c.correct_p());
 }
 

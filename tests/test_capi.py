@@ -105,3 +105,45 @@ def test_ctypes_structs_match_header_layout(ufvm_mod, cname, pyname, tmp_path):
     assert int(got["size"]) == ctypes.sizeof(py)
     for nm, _ in fields:
         assert int(got[nm]) == getattr(py, nm).offset, nm
+
+
+_NULL_CALLS = r'''
+import ctypes as ct, sys
+sys.path.insert(0, ROOT)
+from matlab_ufvm_b200 import ufvm
+L = ufvm.lib()
+S = ufvm._service_lib()
+bad = []
+for lib in (L, S):
+    for name in NAMES:
+        f = getattr(lib, name)
+        types = getattr(f, "argtypes", None)
+        if not types:
+            continue
+        args = []
+        for t in types:
+            if t in (ct.c_int32, ct.c_int, ct.c_int64):
+                args.append(0)
+            elif t in (ct.c_double, ct.c_float):
+                args.append(0.0)
+            else:
+                args.append(None)
+        st = f(*args)
+        if st == 0 and name not in OK_ON_NULL:
+            bad.append((name, st))
+print("BAD", bad)
+'''
+
+
+def test_entry_points_reject_null_handles_and_pointers(ufvm_mod):
+    """Every entry point with declared argument types, called with null handles and pointers
+    and zero sizes, returns a status instead of dereferencing them (run in a child process, so a
+    crash shows as a failure). Only destroy/release of nothing may report success."""
+    import subprocess
+    import sys
+    names = [s for s in declared_symbols() if s not in ("ufvm_version", "ufvm_last_error")]
+    ok_on_null = {"ufvm_case_destroy", "ufvm_service_destroy"}
+    code = f"ROOT = {ROOT!r}\nNAMES = {names!r}\nOK_ON_NULL = {sorted(ok_on_null)!r}\n" + _NULL_CALLS
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "BAD []" in r.stdout, r.stdout
