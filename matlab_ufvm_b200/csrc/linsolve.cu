@@ -805,7 +805,7 @@ int ilu_factor(LinCtx& c, Level& L, int quirks) {
   UFVM_CHECK(c.ensure(L.n));
   UFVM_CHECK(build_schedule(c, L));
   // within one AMG solve the level's matrix is fixed: the factor already computed is the one
-  // the reference recomputes on every smoother call
+  // the reference recomputes on every smoother call (solve/cfdSolveAlgebraicSystem.m:29-33)
   if (c.factor_epoch != 0 && L.dc_epoch == c.factor_epoch && L.dc_quirks == quirks && L.dc.p) return UFVM_OK;
   UFVM_CHECK(dalloc(L.dc, L.n));
   UFVM_CHECK(launch_sweep<OP_ILU_FACT>(c, L, true, quirks));
