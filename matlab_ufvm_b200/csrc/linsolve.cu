@@ -356,7 +356,7 @@ __device__ __forceinline__ void row_op(int i, const SweepArgs& a) {
     }
     __stcg(a.dc + i, 1.0 / d);
   } else if (OP == OP_ILU_FWD) {
-    // solve/cfdSolveILU.m forward substitution over lower j in increasing order
+    // solve/cfdSolveILU.m:33-70 forward substitution over lower j in increasing order
     double v = __ldcg(a.rc + i);
     for (int k = k0; k < k1; k += kChunk) {
       double p[kChunk];
@@ -381,7 +381,7 @@ __device__ __forceinline__ void row_op(int i, const SweepArgs& a) {
       if (done) break;
     }
     __stcg(a.rc + i, v);
-  } else {  // OP_ILU_BWD: backward substitution over upper j in cconn order, then the update
+  } else {  // OP_ILU_BWD (solve/cfdSolveILU.m:72-93): upper j in cconn order, then the update
     double v = __ldcg(a.rc + i);
     if (i < a.n - 1) {
       for (int k = k0; k < k1; k += kChunk) {
