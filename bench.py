@@ -1,32 +1,35 @@
 #!/usr/bin/env python3
 """Converged steady cases per second and p50/p99 time-to-converge of the batched service.
 
-Workload: the batched 2D lid-driven-cavity sweep -- cases with mesh edge n drawn log-uniform
-from 16 to 256 (256 to 65,536 cells) and Re uniform in 50..1000, seeded (seed 2024 gives the
-512-case sweep; the stream continues with seeds 2025, 2026, ... in blocks of 512), steady
-SIMPLE (urf U 0.7, p 0.3, two p correctors), converged to scaled residuals <= 1e-6. The service
-keeps up to --budget cells resident per GPU (continuous batching: a case is admitted as soon as
-cells free up), advances every resident case by one SIMPLE iteration per tick (U: FP64
-multicolour Gauss-Seidel; p: FP32 agglomeration-AMG V-cycle preconditioning FP64 flexible CG),
-and replays each tick as one CUDA graph.
+Workload (the batched-sweep configuration): 512 independent 2D lid-driven cavities, mesh edge n
+drawn log-uniform from 16 to 256 (256 to 65,536 cells) and Re uniform in 50..1000 (seed 2024),
+steady SIMPLE (urf U 0.7, p 0.3, two p correctors), each converged to scaled residuals <= 1e-6.
+All 512 are resident together (about 5.7M cells); every tick advances each unfinished case by
+one SIMPLE iteration (U: FP64 multicolour Gauss-Seidel; p: FP32 agglomeration-AMG V-cycle
+preconditioning FP64 flexible CG) and is replayed as one CUDA graph.
 
-A step is --ticks service ticks. `value` counts the cases that converged during the K timed
-steps, over the device time of those steps (CUDA events on the service's stream, which carry
-the admissions of new cases too; results stay on the device). `e2e` repeats the measurement
-through the public API from host buffers: cases are submitted from host arrays inside the
-timed region, and each converged case's U and p are read back to host and released.
+Timing: a step is --ticks service ticks and the K timed steps cover the whole batch (its slowest
+case needs about 3,500 iterations; the default is 20 steps of 200 ticks), so every case converges
+inside the timed region: `value` = converged cases / device time of the K steps (CUDA events on
+the service's stream). The meshes are uploaded and processed (admission) before the timed region.
+`e2e` repeats the batch through the public API from host buffers: submission from host arrays,
+admission (host-to-device copies), all ticks, and the read-back of every converged case's U and p
+to host memory, timed on the host clock.
 
-Beside it the line carries: the roofline of the dominant kernel (measured live on the resident
-batch), the CPU baseline (the C++ oracle, a serial restatement of the reference's algorithm,
-timed per SIMPLE iteration on host cores and applied to the sweep's iteration counts), and the
-plain FP64 one-case-at-a-time GPU form timed the same way.
+Warm-up: W steps of the same length on a second 512-case batch of the same distribution (seed
+1999). While that batch is resident (inputs larger than L2), the roofline kernels are timed on it.
 
-Multi-GPU: one process per GPU; case i of the stream goes to rank i mod N (independent cases,
-no data-path collective; weak scaling). Timing is the max over ranks.
+Beside the line: the reference arm (`--impl reference`: the C++ oracle, a serial restatement of the
+reference's algorithm, on every host core), the same CPU measurement as `cpu_baseline`, and the
+plain FP64 one-case-at-a-time GPU form.
+
+Multi-GPU: one process per GPU; rank r solves its own 512-case batch (seed 2024 + r): weak scaling,
+no data-path collective. The timed duration is the max over ranks.
 """
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -43,16 +46,17 @@ sys.path.insert(0, ROOT)
 
 SWEEP = 512
 SEED0 = 2024
-ITER_FIXTURE = os.path.join(ROOT, "tests", "golden", "c4_sweep_iterations.json")
+WARM_SEED = 1999
+ORACLE_FIXTURE = os.path.join(ROOT, "tests", "golden", "sweep_oracle.json")
 
 
 def parse():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--ticks", type=int, default=25, help="service ticks per step")
+    ap.add_argument("--ticks", type=int, default=200, help="service ticks per step")
     ap.add_argument("--budget", type=int, default=8_000_000, help="resident cells per GPU")
     ap.add_argument("--admit-interval", type=int, default=8, help="service steps between admissions")
     ap.add_argument("--no-e2e", action="store_true")
@@ -63,8 +67,8 @@ def parse():
                     help="profiling run for ncu: one plain FP64 SIMPLE iteration of a named single-case "
                          "workload inside cudaProfilerStart/Stop (after one warm-up iteration)")
     ap.add_argument("--workload", choices=("sweep", "serving"), default="sweep",
-                    help="sweep: the 2D cavity sweep stream (the headline line); serving: the Poisson-arrival mix "
-                         "of 2D/3D cavities and tet channels (its own JSON line)")
+                    help="sweep: the 512-case 2D cavity batch (the headline line); serving: the Poisson-arrival "
+                         "mix of 2D/3D cavities and tet channels (its own JSON line)")
     ap.add_argument("--serving-requests", type=int, default=48, help="requests per serving phase")
     ap.add_argument("--capacity-steps", type=int, default=400, help="service steps of the closed-loop phase")
     ap.add_argument("--plain-kernels", action="store_true",
@@ -73,20 +77,11 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: eager launches, warm-up only, then one roofline unit of the "
                          "dominant kernel and one step inside cudaProfilerStart/Stop; prints the unit's bytes")
+    ap.add_argument("--profile-cases", type=int, default=128, help="cases resident in the --profile run")
     return ap.parse_args()
 
 
 # ------------------------------------------------------------------ workload
-def stream_params(i: int):
-    from matlab_ufvm_b200 import case
-    b = i // SWEEP
-    key = (b,)
-    if key not in _PARAM_CACHE:
-        _PARAM_CACHE[key] = case.batched_sweep_params(SWEEP, seed=SEED0 + b)
-    return _PARAM_CACHE[key][i % SWEEP]
-
-
-_PARAM_CACHE: dict = {}
 _SPEC_CACHE: dict = {}
 
 
@@ -97,10 +92,14 @@ def base_spec(n: int):
     return _SPEC_CACHE[n]
 
 
-def case_spec(i: int):
-    import dataclasses
-    n, re = stream_params(i)
-    return dataclasses.replace(base_spec(n), nu=1.0 / re, name=f"sweep{i}_n{n}_Re{re:.0f}")
+def batch_params(seed: int, count: int = SWEEP):
+    from matlab_ufvm_b200 import case
+    return case.batched_sweep_params(count, seed=seed)
+
+
+def batch_specs(seed: int, count: int = SWEEP):
+    return [dataclasses.replace(base_spec(n), nu=1.0 / re, name=f"sweep{seed}_{i}_n{n}_Re{re:.0f}")
+            for i, (n, re) in enumerate(batch_params(seed, count))]
 
 
 def _mesh_worker(n):
@@ -108,11 +107,11 @@ def _mesh_worker(n):
     return n, case.cavity_case(n, nu=0.01, quirks=case.QUIRKS_CONVERGING)
 
 
-def prebuild_meshes(indices, ranks: int = 1):
+def prebuild_meshes(sizes, ranks: int = 1):
     """Builds the cavity meshes the run needs in a spawn pool, sharing the host cores with the
     other ranks of the node."""
     import multiprocessing as mp
-    need = sorted({stream_params(i)[0] for i in indices} - set(_SPEC_CACHE))
+    need = sorted(set(sizes) - set(_SPEC_CACHE))
     if not need:
         return
     procs = max(1, min(len(need), (os.cpu_count() or 2) // max(1, ranks) - 1, 32))
@@ -120,8 +119,7 @@ def prebuild_meshes(indices, ranks: int = 1):
         for n in need:
             base_spec(n)
         return
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
+    with mp.get_context("spawn").Pool(procs) as pool:
         for n, spec in pool.imap_unordered(_mesh_worker, sorted(need, reverse=True)):
             _SPEC_CACHE[n] = spec
 
@@ -221,71 +219,80 @@ def gather_list(xs, ws):
     return sharding.gather(xs)
 
 
-# ------------------------------------------------------------------ the service run
-class Feeder:
-    """Keeps the service's queue filled from this rank's share of the case stream."""
-
-    def __init__(self, svc, rank, ws, max_iter=20000, depth=256):
-        self.svc, self.rank, self.ws, self.max_iter, self.depth = svc, rank, ws, max_iter, depth
-        self.k = 0
-        self.queued = 0
-        self.tickets = []
-        self.h2d = 0
-
-    def next_index(self):
-        from matlab_ufvm_b200 import sharding
-        i = sharding.stream_index(self.rank, self.ws, self.k)
-        self.k += 1
-        return i
-
-    def fill(self, n_queued):
-        while n_queued < self.depth:
-            spec = case_spec(self.next_index())
-            self.tickets.append(self.svc.submit(spec, self.max_iter))
-            self.h2d += mesh_bytes(spec)
-            n_queued += 1
+# ------------------------------------------------------------------ the service runs
+MAX_ITER = 20000
+STEP_D2H = 24 * 8 + 4 * 4 + 16  # per resident case and tick: residual scalars and flags read back
 
 
-def run_service(args, rank, ws, e2e: bool):
-    import torch
+def service_settings():
     from matlab_ufvm_b200 import ufvm
-    settings = ufvm.fast_settings(base_spec(16))
-    svc = ufvm.Service(settings, max_resident_cells=args.budget)
+    return ufvm.fast_settings(base_spec(16))
+
+
+def new_service(args):
+    from matlab_ufvm_b200 import ufvm
+    svc = ufvm.Service(service_settings(), max_resident_cells=args.budget)
     svc.set_admit_interval(args.admit_interval)
-    stream = torch.cuda.ExternalStream(svc.stream())
-    feed = Feeder(svc, rank, ws)
-    feed.fill(0)
-    state = {"nr": 0, "nq": feed.depth, "d2h": 0}
-    finished = []  # (ticket, status dict) in completion order
+    return svc
 
-    def tick():
-        nr, nq, nf = svc.step()
-        state["d2h"] += nr * (24 * 8 + 4 * 4 + 16)  # per-step residual scalars and flags read back
-        for t in svc.poll():
-            st = svc.status(t)
-            if e2e:
-                # read the result back to host memory through the public API and free the slot
-                if st["state"] == "converged":
-                    state["d2h"] += svc.field(t, "U").nbytes + svc.field(t, "p").nbytes
-                svc.release(t)
-            finished.append((t, st))
-        feed.fill(nq)
 
+def warm_up(args):
+    """W steps on the warm-up batch; returns the service with that batch still resident."""
+    import torch
+    svc = new_service(args)
+    for s in batch_specs(WARM_SEED):
+        svc.submit(s, MAX_ITER)
+    svc.admit()
     for _ in range(args.warmup * args.ticks):
-        tick()
-    n_before = len(finished)
-    s0 = svc.stats()
-    h2d0, d2h0 = feed.h2d, state["d2h"]
+        nr, nq, _ = svc.step()
+        for t in svc.poll():
+            svc.release(t)
+        if nr == 0 and nq == 0:
+            break
+    torch.cuda.synchronize()
+    return svc
+
+
+def run_batch(args, specs, ws, e2e: bool, rank: int):
+    """The timed batch: every case of `specs` to convergence in K steps of --ticks ticks."""
+    import torch
+    svc = new_service(args)
+    stream = torch.cuda.ExternalStream(svc.stream())
+    h2d = d2h = 0
+    tickets = []
+    if not e2e:
+        tickets = [svc.submit(s, MAX_ITER) for s in specs]
+        svc.admit()
     torch.cuda.synchronize()
     barrier(ws)
     clk = ClockSampler(torch.cuda.current_device()) if rank == 0 and not e2e else None
     if clk:
         clk.start()
+    s0 = svc.stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     w0 = time.perf_counter()
-    for _ in range(args.steps * args.ticks):
-        tick()
+    if e2e:
+        for s in specs:
+            tickets.append(svc.submit(s, MAX_ITER))
+            h2d += mesh_bytes(s)
+    finished = {}
+    remaining = len(specs)
+    for _ in range(args.steps):
+        for _ in range(args.ticks):
+            if remaining == 0:
+                break
+            nr, nq, _ = svc.step()
+            d2h += nr * STEP_D2H
+            for t in svc.poll():
+                st = svc.status(t)
+                if e2e:
+                    if st["state"] == "converged":
+                        u, p = svc.field(t, "U"), svc.field(t, "p")
+                        d2h += u.nbytes + p.nbytes
+                    svc.release(t)
+                finished[t] = st
+                remaining -= 1
     ev1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - w0
@@ -293,38 +300,56 @@ def run_service(args, rank, ws, e2e: bool):
     barrier(ws)
     clocks = clk.stop() if clk else None
     s1 = svc.stats()
-    win = [st for _, st in finished[n_before:] if st["state"] == "converged"]
-    out = dict(ms=ms, wall=wall, converged=len(win), ttc=[st["latency_ms"] for st in win],
-               queue=[st["queue_ms"] for st in win], iters=[st["iterations"] for st in win],
-               stopped=sum(1 for _, st in finished[n_before:] if st["state"] != "converged"),
+    conv = [st for st in finished.values() if st["state"] == "converged"]
+    out = dict(ms=ms, wall=wall, converged=len(conv), cases=len(specs), complete=remaining == 0,
+               ttc=[st["latency_ms"] for st in conv], iters=[st["iterations"] for st in conv],
+               stopped=sum(1 for st in finished.values() if st["state"] != "converged"),
                launches=s1["graph_launches"] - s0["graph_launches"],
                graph_ticks=s1["graph_ticks"] - s0["graph_ticks"], ticks=s1["steps"] - s0["steps"],
-               captures=s1["captures"] - s0["captures"],
-               h2d=feed.h2d - h2d0, d2h=state["d2h"] - d2h0, clocks=clocks)
+               captures=s1["captures"] - s0["captures"], slot_drops=s1["slot_drops"] - s0["slot_drops"],
+               peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
+               tickets=tickets)
     return svc, out
 
 
 ROOF_KERNEL = (1, "k_mc32_l0 (FP32 multicolour Gauss-Seidel sweep of the V-cycle's level 0, "
                   "colour-permuted ELL; one unit = both colours forward then backward over every case)")
 
+# Units of the service's profiling hook: (id, name, units per tick as a function of the tick's U
+# smoother sweeps and p V-cycles, bound)
+TICK_UNITS = (
+    (0, "k_mc64_items (FP64 multicolour Gauss-Seidel sweep of U, ELL copy)", lambda us, pc: us, "hbm"),
+    (1, "k_mc32_l0 (FP32 multicolour Gauss-Seidel sweep of the V-cycle's level 0, pre and post)",
+     lambda us, pc: 2 * pc, "hbm"),
+    (2, "k_fcg_q (FP64 q = A p with (p, q) and (p, r), one per V-cycle)", lambda us, pc: pc, "hbm"),
+    (6, "k_coarse_vcycle_pk (the levels below the grid levels, one CTA per large case or 4 small ones)",
+     lambda us, pc: pc, "latency"),
+    (3, "k_uface + k_assemble_u + k_du_boundary (momentum assembly, 3 components)", lambda us, pc: 3, "hbm"),
+    (4, "k_rhiechow + k_assemble_p (Rhie-Chow face flux and p matrix, 2 correctors)", lambda us, pc: 2, "hbm"),
+    (5, "k_bc_update + k_grad_cells + k_grad_bfix + k_minmax_U (field update: gradients of U and p)",
+     lambda us, pc: 1, "hbm"),
+)
+
 
 def main_profile(args):
     """ncu target: the kernels of one unit of the roofline kernel and of one eager step."""
     import torch
-    from matlab_ufvm_b200 import build as _b, ufvm
+    from matlab_ufvm_b200 import build as _b
     torch.cuda.set_device(0)
     _b.build()
-    # meshes are built on demand in this process (no worker pool under the profiler)
-    settings = ufvm.fast_settings(base_spec(16))
+    settings = service_settings()
     settings.service_eager = 1
+    from matlab_ufvm_b200 import ufvm
     svc = ufvm.Service(settings, max_resident_cells=args.budget)
     svc.set_schedule(8192)
-    feed = Feeder(svc, 0, 1)
-    feed.fill(0)
+    for s in batch_specs(WARM_SEED, args.profile_cases):
+        svc.submit(s, MAX_ITER)
+    svc.admit()
+    nr = 0
     for _ in range(args.warmup * args.ticks):
-        nr, nq, nf = svc.step()
-        svc.poll()
-        feed.fill(nq)
+        nr, nq, _ = svc.step()
+        for t in svc.poll():
+            svc.release(t)
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
     ms, by = svc.profile(ROOF_KERNEL[0], 1)
@@ -359,24 +384,44 @@ def main_profile_plain(args):
     return 0
 
 
-def roofline(svc, peaks):
-    """Dominant kernel, timed live on the resident batch."""
-    kernel_id, name = ROOF_KERNEL
-    ms, by = svc.profile(kernel_id, 20)
-    achieved = by / (ms * 1e-3) / 1e9
+def roofline(svc, peaks, ticks: int = 12):
+    """Every major kernel of the tick, timed live on the resident batch with CUDA events (the
+    service's profiling hook), with its share of the measured tick; the line's roofline is the
+    largest of them. Leaves the batch fit only for timing (the assembly units rewrite fields)."""
+    import torch
+    stream = torch.cuda.ExternalStream(svc.stream())
+    s0 = svc.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ticks):
+        svc.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    s1 = svc.stats()
+    gt = max(1, s1["graph_ticks"] - s0["graph_ticks"])
+    tick_ms = e0.elapsed_time(e1) / ticks
+    us = (s1["u_loop_bodies"] - s0["u_loop_bodies"]) / gt
+    pc = (s1["p_loop_bodies"] - s0["p_loop_bodies"]) / gt
     peak = peaks.get("hbm_gbs")
-    others = []
-    for kid, kname in ((0, "k_mc64 (FP64 multicolour Gauss-Seidel sweep of U, ELL copy)"),
-                       (2, "k_fcg_q (FP64 q = A p with (p, q) and (p, r))")):
-        m2, b2 = svc.profile(kid, 20)
-        a2 = b2 / (m2 * 1e-3) / 1e9
-        others.append({"kernel": kname, "achieved": round(a2, 1), "frac": round(a2 / peak, 4) if peak else None,
-                       "bytes_per_unit": b2, "ms_per_unit": round(m2, 4)})
-    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4) if peak else None, "traffic": None,
-            "bytes_per_unit": by, "ms_per_unit": round(ms, 4),
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peak else "unavailable (fallback)",
-            "other_kernels": others}
+    rows = []
+    for kid, name, per_tick, bound in TICK_UNITS:
+        ms, by = svc.profile(kid, 10)
+        a = by / (ms * 1e-3) / 1e9
+        t = ms * per_tick(us, pc)
+        rows.append({"kernel": name, "bound": bound, "ms_per_unit": round(ms, 4), "bytes_per_unit": by,
+                     "achieved": round(a, 1), "frac": round(a / peak, 4) if peak else None,
+                     "units_per_tick": round(per_tick(us, pc), 2), "ms_per_tick": round(t, 3),
+                     "share_of_tick": round(t / tick_ms, 4) if tick_ms > 0 else None})
+    top = max(rows, key=lambda r: r["ms_per_tick"])
+    top_hbm = max((r for r in rows if r["bound"] == "hbm"), key=lambda r: r["ms_per_tick"])
+    return {"kernel": top_hbm["kernel"], "bound": "hbm", "achieved": top_hbm["achieved"], "peak": peak,
+            "unit": "GB/s", "frac": top_hbm["frac"], "traffic": None, "bytes_per_unit": top_hbm["bytes_per_unit"],
+            "ms_per_unit": top_hbm["ms_per_unit"], "share_of_tick": top_hbm["share_of_tick"],
+            "largest_kernel_of_tick": top["kernel"],
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if not peaks.get("fallback")
+            else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)",
+            "tick_ms": round(tick_ms, 3), "u_sweeps_per_tick": round(us, 2), "p_cycles_per_tick": round(pc, 2),
+            "resident_cases": s1.get("resident_cases"), "kernels": rows}
 
 
 def load_peaks():
@@ -399,105 +444,204 @@ def load_peaks():
     return out
 
 
-# ------------------------------------------------------------------ per-iteration cost models
-SAMPLE_N = (16, 24, 32, 48, 64, 96, 128, 192, 256)
+# ------------------------------------------------------------------ the CPU arm (the oracle)
+def oracle_fixture():
+    """The oracle on a stratified 64-case sample of the batch, converged on the machine that wrote
+    the fixture: its own iteration counts and seconds to each residual decade."""
+    with open(ORACLE_FIXTURE) as f:
+        d = json.load(f)
+    d["sample_cases"] = [c for c in d["cases"] if c["sample"]]
+    return d
 
 
-def sweep_iterations():
-    """Iterations to converge of the 512 sweep cases (service, same SIMPLE settings)."""
-    d = json.load(open(ITER_FIXTURE))
-    return [(int(c["n"]), int(c["iterations"])) for c in d["cases"]]
-
-
-def interp_cost(samples: dict, n: int) -> float:
-    """log-log interpolation of seconds per iteration over the sampled sizes."""
-    xs = sorted(samples)
-    if n <= xs[0]:
-        return samples[xs[0]] * (n / xs[0]) ** 2
-    if n >= xs[-1]:
-        return samples[xs[-1]] * (n / xs[-1]) ** 2
-    for a, b in zip(xs, xs[1:]):
-        if a <= n <= b:
-            la, lb = math.log(samples[a]), math.log(samples[b])
-            f = (math.log(n) - math.log(a)) / (math.log(b) - math.log(a))
-            return math.exp(la + f * (lb - la))
-    return samples[xs[-1]]
-
-
-def _oracle_sample(arg):
-    """Seconds per SIMPLE iteration of the oracle (one core) on a cavity of edge n."""
-    n, budget_s = arg
+def _oracle_first3(arg):
+    """Seconds of the first three SIMPLE iterations of the oracle (one core) on a batch case."""
+    n, re = arg
     from matlab_ufvm_b200 import case
     from oracle import oracle
-    spec = case.cavity_case(n, nu=1.0 / 500.0, quirks=case.QUIRKS_CONVERGING)
+    spec = case.cavity_case(n, nu=1.0 / re, quirks=case.QUIRKS_CONVERGING, tol_u=0.0, tol_p=0.0)
     oc = oracle.OracleCase(spec)
-    oc.iterate()  # warm-up
     t0 = time.perf_counter()
-    k = 0
-    while True:
+    for _ in range(3):
         oc.iterate()
-        k += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or k >= 20:
-            break
-    return n, el / k, k
+    return time.perf_counter() - t0
 
 
-def cpu_baseline(workers: int, budget_s: float):
-    """Oracle cost per iteration at the sample sizes, all workers busy at once (spawn pool)."""
+def _oracle_converge(arg):
+    """The oracle to convergence (residualControl 1e-6) on one core: (seconds, iterations, state)."""
+    n, re = arg
+    from matlab_ufvm_b200 import case
+    from oracle import oracle
+    spec = case.cavity_case(n, nu=1.0 / re, quirks=case.QUIRKS_CONVERGING)
+    oc = oracle.OracleCase(spec)
+    t0 = time.perf_counter()
+    for it in range(1, MAX_ITER + 1):
+        rc, _ = oc.iterate()
+        if rc != 0:
+            return time.perf_counter() - t0, it, "converged" if rc == 1 else "diverged"
+    return time.perf_counter() - t0, MAX_ITER, "stopped"
+
+
+def cpu_batch_estimate(pool, workers: int, fix) -> dict:
+    """Converged cases/s of the 512-case batch on `workers` host cores, one case per core.
+
+    Each of the 64 sample cases (every 8th case of the batch ranked by n) contributes its measured
+    single-core time to converge, taken from the fixture's full run and carried to this machine by
+    the ratio of the first three iterations timed here now (all workers busy, as in the batch) to
+    the same iterations on the fixture's machine. A case on which the oracle diverged contributes
+    the time it ran until the divergence and no converged case. The batch's total is 512/64 of the
+    sample's; the cores are assumed perfectly packed (the longest case alone is far shorter than
+    total / cores), which favours the CPU."""
+    sample = fix["sample_cases"]
+    t3 = pool.map(_oracle_first3, [(c["n"], c["re"]) for c in sample])
+    times, conv, ratios = [], 0, []
+    for c, t in zip(sample, t3):
+        ratio = t / c["seconds_first3"]
+        ratios.append(ratio)
+        if "diverged_at" in c or "6" not in c.get("seconds_to", {}):
+            times.append(c["seconds"] * ratio)
+        else:
+            times.append(c["seconds_to"]["6"] * ratio)
+            conv += 1
+    total = sum(times) * SWEEP / len(sample)
+    wall = max(total / workers, max(times))
+    converged = SWEEP * conv / len(sample)
+    return {"cases_per_s": converged / wall, "batch_seconds": wall, "converged_cases": converged,
+            "core_seconds": total, "sample_cases": len(sample), "sample_converged": conv,
+            "speed_ratio_median": statistics.median(ratios),
+            "sample_time_s": sum(t3), "per_case": times}
+
+
+def cpu_model_check(pool, fix, est: dict, limit_s: float = 3.0) -> dict:
+    """Converges the sample cases whose predicted time is under `limit_s` on this machine and
+    compares the measured seconds with the prediction of cpu_batch_estimate."""
+    pick = [(c, p) for c, p in zip(fix["sample_cases"], est["per_case"])
+            if p < limit_s and "diverged_at" not in c and "6" in c.get("first", {})]
+    res = pool.map(_oracle_converge, [(c["n"], c["re"]) for c, _ in pick])
+    rows = []
+    for (c, pred), (sec, it, state) in zip(pick, res):
+        rows.append({"n": c["n"], "re": round(c["re"], 1), "iterations": it, "fixture_iterations": c["first"]["6"],
+                     "measured_s": round(sec, 4), "predicted_s": round(pred, 4), "state": state})
+    ratios = [r["measured_s"] / r["predicted_s"] for r in rows if r["predicted_s"] > 0]
+    return {"cases": len(rows), "iterations_match": all(r["iterations"] == r["fixture_iterations"] for r in rows),
+            "measured_over_predicted": {"median": statistics.median(ratios) if ratios else None,
+                                        "min": min(ratios) if ratios else None,
+                                        "max": max(ratios) if ratios else None},
+            "measured_total_s": round(sum(r["measured_s"] for r in rows), 3),
+            "predicted_total_s": round(sum(r["predicted_s"] for r in rows), 3)}
+
+
+def cpu_workers(args) -> int:
+    return args.cpu_workers or min(os.cpu_count() or 1, 64)
+
+
+def cpu_sample_text(workers, est) -> str:
+    return (f"C++ oracle (serial restatement of the reference's SIMPLE loop with its own V-cycle AMG + "
+            f"Gauss-Seidel for p and DILU for U) on {workers} concurrent processes: the first 3 SIMPLE "
+            f"iterations of each of the {est['sample_cases']} stratified sample cases of the 512-case batch "
+            f"timed here, scaled to each case's fully measured single-core time to convergence "
+            f"(tests/golden/sweep_oracle.json; median speed ratio here/there {est['speed_ratio_median']:.3f}); "
+            f"{est['sample_converged']}/{est['sample_cases']} sample cases converge in the oracle; "
+            f"batch total / cores, perfectly packed")
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def workload_config(args):
+    return {"workload": "512-case batched 2D lid-driven cavity sweep: n log-uniform 16..256 (256-65,536 cells), "
+                        "Re uniform 50..1000, seed 2024 (rank r: 2024 + r), SIMPLE to scaled residuals 1e-6, "
+                        "every case converged inside the timed region",
+            "cases_per_gpu": SWEEP, "ticks_per_step": args.ticks, "resident_cells_per_gpu_cap": args.budget,
+            "l2": "inputs larger than L2 (about 5.7M resident cells, GBs of matrices and fields)",
+            "parallelism": f"case-sharded x{args.gpus} (one batch per GPU)"}
+
+
+# ------------------------------------------------------------------ arms
+def main_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
     import multiprocessing as mp
     from oracle import oracle
     oracle.build()
-    ctx = mp.get_context("spawn")
-    jobs = [(n, budget_s) for n in SAMPLE_N]
-    jobs = (jobs * ((workers + len(jobs) - 1) // len(jobs)))[:max(workers, len(jobs))]
-    t0 = time.perf_counter()
-    with ctx.Pool(workers) as pool:
-        res = pool.map(_oracle_sample, jobs)
-    wall = time.perf_counter() - t0
-    per = {}
-    for n, s, k in res:
-        per.setdefault(n, []).append(s)
-    samples = {n: statistics.median(v) for n, v in per.items()}
-    its = sweep_iterations()
-    seconds_per_case = statistics.mean(it * interp_cost(samples, n) for n, it in its)
-    return {"cases_per_s": workers / seconds_per_case, "s_per_iter": samples, "wall": wall,
-            "seconds_per_case": seconds_per_case}
-
-
-def plain_gpu_sample(budget_s: float):
-    """The plain FP64 form (reference smoothers, AMG rebuilt every p solve) one case at a time."""
-    import torch
-    from matlab_ufvm_b200 import case, ufvm
-    samples = {}
-    for n in (16, 32, 64, 128, 256):
-        spec = case.cavity_case(n, nu=1.0 / 500.0, quirks=case.QUIRKS_CONVERGING)
-        g = ufvm.GpuCase(spec)
-        g.iterate()
-        torch.cuda.synchronize()
+    fix = oracle_fixture()
+    workers = cpu_workers(args)
+    with mp.get_context("spawn").Pool(workers) as pool:
+        check = None
+        for w in range(args.warmup):
+            est = cpu_batch_estimate(pool, workers, fix)
+            if w == 0:
+                check = cpu_model_check(pool, fix, est)
+        vals = []
         t0 = time.perf_counter()
-        k = 0
-        while True:
-            g.iterate()
-            k += 1
-            if time.perf_counter() - t0 > budget_s / 5 or k >= 10:
-                break
-        torch.cuda.synchronize()
-        samples[n] = (time.perf_counter() - t0) / k
-        g.close()
-    its = sweep_iterations()
-    seconds_per_case = statistics.mean(it * interp_cost(samples, n) for n, it in its)
-    return {"cases_per_s": 1.0 / seconds_per_case, "s_per_iter": samples, "seconds_per_case": seconds_per_case}
+        for _ in range(args.steps):
+            est = cpu_batch_estimate(pool, workers, fix)
+            vals.append(est["cases_per_s"])
+        el = time.perf_counter() - t0
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "converged_cases_per_s", "value": v, "unit": "cases/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": v, "unit": "cases/s", "cores": workers, "kind": "port",
+                         "sample": cpu_sample_text(workers, est)},
+        "e2e": {"value": v, "unit": "cases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "batch_seconds": est["batch_seconds"], "converged_cases": est["converged_cases"],
+        "model_check": check,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
 
 
-def plain_kernel_rooflines(peaks):
+def _plain_first3(spec):
+    import torch
+    from matlab_ufvm_b200 import ufvm
+    g = ufvm.GpuCase(spec)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        g.iterate()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    g.close()
+    return el
+
+
+def plain_batch_estimate(fix, here_t3: list) -> dict:
+    """The plain FP64 form (the reference's solvers, bit-exact with the oracle, so with the oracle's
+    iteration counts) one case at a time: each sample case's first three iterations are timed on
+    the GPU and scaled by the fixture's measured time to convergence over its first three
+    iterations' time; the batch's total is 512/64 of the sample's."""
+    from matlab_ufvm_b200 import case
+    sample = fix["sample_cases"]
+    _plain_first3(case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING))  # warm the path
+    times, conv, per_iter = [], 0, {}
+    for c in sample:
+        spec = dataclasses.replace(base_spec(c["n"]), nu=1.0 / c["re"], tol_u=0.0, tol_p=0.0)
+        t3 = _plain_first3(spec)
+        per_iter[str(c["n"])] = round(t3 / 3, 6)
+        ratio = t3 / c["seconds_first3"]
+        if "diverged_at" in c or "6" not in c.get("seconds_to", {}):
+            times.append(c["seconds"] * ratio)
+        else:
+            times.append(c["seconds_to"]["6"] * ratio)
+            conv += 1
+    total = sum(times) * SWEEP / len(sample)
+    return {"cases_per_s": SWEEP * conv / len(sample) / total, "batch_seconds": total,
+            "s_per_iter_first3": per_iter}
+
+
+def plain_kernel_rooflines(peaks, spec=None):
     """The plain FP64 form's solver kernels on the 1,029,000-cell tet channel's momentum matrix
     (device arrays), kernel time only: the library's profiling entry point prepares schedules,
     colourings and the DILU factor, then times each launch with CUDA events after a read of
     twice the L2 size."""
     import torch
     from matlab_ufvm_b200 import case, ufvm
-    spec = case.channel_case()
+    spec = spec or case.channel_case()
     g = ufvm.GpuCase(spec)
     g.iterate()
     g.cfdUpdateFields()
@@ -523,7 +667,7 @@ def plain_kernel_rooflines(peaks):
     return out
 
 
-def plain_named_configs():
+def plain_named_configs(channel=None):
     """Seconds per steady SIMPLE iteration of the plain FP64 form on the named single-case
     workloads, on the GPU and in the oracle (one host core), same settings as the reference's
     tutorials: the 20x20 cavity (Re 100), the 64^3 cavity (Re 400, ILU for p) and the
@@ -535,8 +679,8 @@ def plain_named_configs():
     out = {}
     for key, make, n_gpu, n_cpu in (
             ("C1_cavity_20x20", lambda: case.cavity_case(20, nu=0.01), 10, 10),
-            ("C2_cavity_64cubed_ilu", lambda: case.cavity_case(64, nu=1.0 / 400, dim=3, p_smoother="ILU"), 4, 2),
-            ("C3_channel_1M_tet", lambda: case.channel_case(), 3, 1)):
+            ("C2_cavity_64cubed_ilu", lambda: case.cavity_case(64, nu=1.0 / 400, dim=3, p_smoother="ILU"), 2, 1),
+            ("C3_channel_1M_tet", lambda: channel or case.channel_case(), 1, 1)):
         spec = make()
         g = ufvm.GpuCase(spec)
         g.iterate()
@@ -560,52 +704,6 @@ def plain_named_configs():
     return out
 
 
-def pct(v, q):
-    return float(np.percentile(np.asarray(v), q)) if len(v) else None
-
-
-# ------------------------------------------------------------------ arms
-def main_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
-    workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
-    budget = 2.0
-    for _ in range(args.warmup):
-        cpu_baseline(workers, 0.3)
-    vals = []
-    last = None
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        last = cpu_baseline(workers, budget)
-        vals.append(last["cases_per_s"])
-    el = time.perf_counter() - t0
-    v = statistics.median(vals)
-    line = {
-        "impl": "reference", "metric": "converged_cases_per_s", "value": v, "unit": "cases/s",
-        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args),
-        "cpu_baseline": {"value": v, "unit": "cases/s", "cores": workers, "kind": "port",
-                         "sample": f"C++ oracle (serial restatement of the reference SIMPLE/AMG loop), "
-                                   f"seconds per SIMPLE iteration at n in {list(SAMPLE_N)} "
-                                   f"(Re 500) on {workers} concurrent processes, applied to the 512 sweep "
-                                   f"cases' iteration counts; {workers} cases in parallel"},
-        "e2e": {"value": v, "unit": "cases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "s_per_iter": {str(k): round(s, 6) for k, s in last["s_per_iter"].items()},
-    }
-    print(json.dumps(line), flush=True)
-    return 0
-
-
-def workload_config(args):
-    return {"workload": "2D lid-driven cavity sweep stream: n log-uniform 16..256, Re uniform 50..1000, "
-                        "seeds 2024+ (first 512 = the batched sweep), SIMPLE to scaled residual 1e-6",
-            "resident_cells_per_gpu": args.budget, "ticks_per_step": args.ticks,
-            "l2": "inputs larger than L2 (resident batch of up to ~6M cells, GBs of matrices and fields)",
-            "parallelism": f"case-sharded x{args.gpus}"}
-
-
 def main_ours(args):
     import torch
     rank, ws, local = dist_setup(args) if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 \
@@ -615,39 +713,50 @@ def main_ours(args):
         return 1
     if ws == 1:
         torch.cuda.set_device(0)
-    from matlab_ufvm_b200 import build as _b
+    from matlab_ufvm_b200 import build as _b, sharding
     _b.build()
-    # meshes for the first cases of this rank's share (the rest are built on demand)
-    from matlab_ufvm_b200 import sharding
-    prebuild_meshes([sharding.stream_index(rank, ws, k) for k in range(1200 // ws + 1)], ws)
+    seed = sharding.batch_seed(rank, ws, SEED0)
+    prebuild_meshes([n for n, _ in batch_params(seed)] + [n for n, _ in batch_params(WARM_SEED)], ws)
+    specs = batch_specs(seed)
     peaks = load_peaks()
-    svc, res = run_service(args, rank, ws, e2e=False)
-    roof = roofline(svc, peaks) if rank == 0 else None
+    wsvc = warm_up(args)
+    roof = roofline(wsvc, peaks) if rank == 0 else None
+    wsvc.close()
+    svc, res = run_batch(args, specs, ws, e2e=False, rank=rank)
     svc.close()
     total = reduce_sum(res["converged"], ws)
     ms = reduce_max(res["ms"], ws)
     value = total / (ms * 1e-3) if ms > 0 else 0.0
     ttc = gather_list(res["ttc"], ws)
-    qms = gather_list(res["queue"], ws)
+    iters = gather_list(res["iters"], ws)
     e2e = None
     if not args.no_e2e:
-        svc2, r2 = run_service(args, rank, ws, e2e=True)
+        svc2, r2 = run_batch(args, specs, ws, e2e=True, rank=rank)
         svc2.close()
         tot2 = reduce_sum(r2["converged"], ws)
-        ms2 = reduce_max(r2["ms"], ws)
-        e2e = {"value": tot2 / (ms2 * 1e-3) if ms2 > 0 else 0.0, "unit": "cases/s",
+        wall2 = reduce_max(r2["wall"], ws)
+        e2e = {"value": tot2 / wall2 if wall2 > 0 else 0.0, "unit": "cases/s",
                "h2d_bytes_per_step": int(reduce_sum(r2["h2d"], ws) / args.steps),
                "d2h_bytes_per_step": int(reduce_sum(r2["d2h"], ws) / args.steps),
-               "wall_s": round(r2["wall"], 3)}
-    plain = cpu = None
+               "wall_s": round(r2["wall"], 3), "device_s": round(r2["ms"] * 1e-3, 3),
+               "complete": bool(r2["complete"])}
+    plain = cpu = check = None
     if rank == 0 and ws == 1:
+        fix = oracle_fixture() if os.path.exists(ORACLE_FIXTURE) else None
+        if not args.no_cpu and fix:
+            import multiprocessing as mp
+            from oracle import oracle
+            oracle.build()
+            workers = cpu_workers(args)
+            with mp.get_context("spawn").Pool(workers) as pool:
+                cpu = cpu_batch_estimate(pool, workers, fix)
+            cpu["workers"] = workers
         if not args.no_plain:
-            plain = plain_gpu_sample(20.0)
-            plain["kernels"] = plain_kernel_rooflines(peaks)
-            plain["named"] = plain_named_configs()
-        if not args.no_cpu:
-            workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
-            cpu = cpu_baseline(workers, 2.0)
+            from matlab_ufvm_b200 import case
+            plain = plain_batch_estimate(fix, None) if fix else {}
+            channel = case.channel_case()
+            plain["kernels"] = plain_kernel_rooflines(peaks, channel)
+            plain["named"] = plain_named_configs(channel)
     launches = int(reduce_sum(res["launches"], ws))
     if rank == 0:
         line = {
@@ -656,28 +765,31 @@ def main_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
             "data": "synthetic (seeded cavity meshes generated in-process)",
             "config": workload_config(args),
+            "batch_complete": bool(res["complete"]), "converged": int(total), "cases": SWEEP * ws,
+            "stopped": int(reduce_sum(res["stopped"], ws)),
             "time_to_converge_ms": {"p50": pct(ttc, 50), "p99": pct(ttc, 99), "n": len(ttc),
                                     "clock": "service device clock, admission to convergence"},
-            "queue_ms": {"p50": pct(qms, 50), "p99": pct(qms, 99)},
-            "converged_in_window": int(total), "stopped_in_window": int(reduce_sum(res["stopped"], ws)),
+            "iterations": {"p50": pct(iters, 50), "max": max(iters) if iters else None},
             "ticks_timed": res["ticks"], "graph_ticks": res["graph_ticks"], "graph_captures": res["captures"],
+            "slot_drops": res["slot_drops"], "resident_bytes_end": res["peak_bytes"],
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res["clocks"],
         }
         if cpu:
             line["cpu_baseline"] = {
-                "value": cpu["cases_per_s"], "unit": "cases/s", "cores": args.cpu_workers or min(os.cpu_count() or 1, 64),
-                "kind": "port",
-                "sample": "C++ oracle seconds per SIMPLE iteration at n in %s (Re 500, 2 s each), applied to the "
-                          "512 sweep cases' iteration counts" % (list(SAMPLE_N),),
-                "s_per_iter": {str(k): round(s, 6) for k, s in cpu["s_per_iter"].items()}}
+                "value": cpu["cases_per_s"], "unit": "cases/s", "cores": cpu["workers"], "kind": "port",
+                "sample": cpu_sample_text(cpu["workers"], cpu), "batch_seconds": round(cpu["batch_seconds"], 1)}
         if plain:
             line["plain_fp64_gpu"] = {
-                "value": plain["cases_per_s"], "unit": "cases/s",
-                "method": "plain FP64 form (reference SOR/ILU smoothers, AMG rebuilt every p solve) one case at a "
-                          "time: seconds per SIMPLE iteration at n in 16..256 applied to the sweep's iteration counts",
-                "s_per_iter": {str(k): round(s, 6) for k, s in plain["s_per_iter"].items()},
+                "value": plain.get("cases_per_s"), "unit": "cases/s",
+                "method": "plain FP64 form (the reference's V-cycle + Gauss-Seidel for p and DILU for U, AMG rebuilt "
+                          "every p solve, bit-exact with the oracle) one case at a time: each sample case's first "
+                          "3 iterations timed on the GPU, scaled by the oracle fixture's measured time to "
+                          "convergence over its first 3 iterations",
+                "batch_seconds": plain.get("batch_seconds"),
+                "s_per_iter_first3": plain.get("s_per_iter_first3"),
                 "kernels_1M_tet_channel": plain["kernels"], "named_configs": plain["named"]}
-            line["batched_over_plain"] = value / plain["cases_per_s"] if plain["cases_per_s"] else None
+            if plain.get("cases_per_s"):
+                line["batched_over_plain"] = value / plain["cases_per_s"]
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -697,7 +809,6 @@ def main_serving(args):
     the capacity in converged cases per second of service clock; an open-loop phase on a fresh
     service then submits a second seeded stream at Poisson arrival times of 0.8 x that rate and
     reports throughput and time-to-converge percentiles from arrival."""
-    import dataclasses
     import multiprocessing as mp
     import torch
     from matlab_ufvm_b200 import build as _b, serving, ufvm
@@ -715,7 +826,7 @@ def main_serving(args):
     def spec_fn(req):
         return dataclasses.replace(base[(req.kind, req.size)], nu=1.0 / req.re, name=f"serving{req.index}")
 
-    settings = ufvm.fast_settings(base_spec(16))
+    settings = service_settings()
 
     def service():
         svc = ufvm.Service(settings, max_resident_cells=args.budget)
@@ -724,6 +835,9 @@ def main_serving(args):
 
     svc = service()
     cap = serving.closed_loop_capacity(svc, cap_reqs, args.capacity_steps, spec_fn=spec_fn)
+    cap["stats"] = {k: v for k, v in svc.stats().items() if k in ("resident_bytes", "memory_budget",
+                                                                  "deferred_for_memory", "oom_requeues",
+                                                                  "footprint_scale", "captures", "slot_drops")}
     svc.close()
     rate = 0.8 * cap["cases_per_s"]
     line = {"workload": "serving mix (70% 2D cavities 1k-64k cells, 25% 3D cavities 32^3-96^3, 5% tet channels "
@@ -734,6 +848,9 @@ def main_serving(args):
         arr = serving.poisson_arrivals(len(open_reqs), rate, seed=303)
         ol = serving.OpenLoop(svc, open_reqs, arr, spec_fn=spec_fn)
         out = ol.run()
+        line["open_loop_stats"] = {k: v for k, v in svc.stats().items() if k in (
+            "resident_bytes", "memory_budget", "deferred_for_memory", "oom_requeues", "footprint_scale",
+            "captures", "slot_drops", "steps")}
         svc.close()
         line.update(metric="converged cases/s + p50/p99 time to converge (from arrival, service clock)",
                     open_loop=serving.summarize(out), service_steps=ol.steps, idle_s=ol.idle_s)

@@ -172,6 +172,8 @@ int ufvm_solve_sor(int32_t n, const int32_t* rowptr, const int32_t* col, const d
  * its scratch lives in one fixed array of about 4 MiB compiled into the library, so systems of
  * more than 262,144 rows are rejected with UFVM_E_INVALID. Every call shares that array and
  * clears what it needs; calls whose device work overlaps race on it and must be serialised.
+ * The matrix must be structurally symmetric (every finite-volume matrix is), as for
+ * ufvm_solve_sor: the level schedule is built from each row's lower neighbours.
  * The first call on a device looks the array up with cudaGetSymbolAddress: make it before any
  * stream capture. Results are bit-identical to ufvm_solve_sor's. */
 int ufvm_solve_sor_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
@@ -211,10 +213,17 @@ int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col,
                            int32_t* n_coarse, int32_t* nnz_coarse, void* stream);
 
 /* ---- batched steady-case service (continuous batching of independent cases) ----
- * Cases are admitted first-come first-served while the resident-cell budget allows, every
+ * Cases are admitted first-come first-served while their HBM footprint fits the memory budget
+ * (ufvm_service_set_memory_budget; by default 90% of the device memory free at creation) and
+ * their cells fit max_resident_cells. A queued case's footprint is estimated from its face,
+ * interior-face and cell counts, scaled by the largest ratio of measured to estimated bytes the
+ * service has seen; a resident case counts its measured allocations. A case that fails to
+ * allocate at admission waits at the head of the queue while other cases are resident. Every
  * resident case advances one SIMPLE iteration per ufvm_service_step in one launch per stage,
- * and a case leaves the resident set when it converges (residualControl), fails, or reaches
- * its iteration limit, freeing room for queued cases. The solver settings are shared by all
+ * and a case finishes when it converges (residualControl), fails, or reaches its iteration
+ * limit; its result (U, p, mdot at that iteration) is kept on the device until release, and its
+ * own memory is freed when its slot leaves the batch (gathered with the next admission, or when
+ * finished slots reach 1/16 of the active cells or 32 steps), freeing room for queued cases. The solver settings are shared by all
  * cases of a service; nu, the boundary data and the pressure reference cell are per case (a
  * case whose boundaries are all walls, empty or symmetry planes pins p at settings->
  * fixed_element, or cell 0 if that is negative; any other case has none, cfdReadSystem.m:
@@ -238,8 +247,23 @@ int ufvm_service_release(ufvm_service* s, int64_t ticket);
  * then the number of U smoother sweeps, p V-cycles, steps, the service clock (ms), the ticks
  * replayed as a captured graph, the number of graph captures and the kernel launches executed by
  * the replayed graphs (loop bodies counted per execution), the current CTA threshold of the
- * V-cycle and the number of completed autotuning passes. Writes min(n, 17) values. */
+ * V-cycle, the number of completed autotuning passes, the HBM bytes held by the slots and the
+ * unreleased results, the memory budget, the admissions deferred for memory, the admissions
+ * that failed to allocate and were re-queued, the departures of finished slots from the batch,
+ * the footprint estimate's scale, and the U-smoother and p-cycle loop bodies the replayed ticks
+ * have run. Writes min(n, 25) values. */
 int ufvm_service_stats(ufvm_service* s, double* out, int n);
+/* Admits queued cases now, as far as the budgets allow, without waiting for the next step: their
+ * meshes are uploaded and processed on the service stream, so a caller can have a batch resident
+ * on the device before it starts timing or stepping. *n_resident: active cases afterwards. */
+int ufvm_service_admit(ufvm_service* s, int32_t* n_resident);
+/* Fault injection for tests (no counterpart in the reference): the next `count` admissions of
+ * `ticket` fail as if a device allocation had failed (UFVM_E_OOM), without allocating. While
+ * other cases are resident such a request waits at the head of the queue; on an empty service
+ * it is stopped with UFVM_E_OOM. */
+int ufvm_service_inject_admit_oom(ufvm_service* s, int64_t ticket, int32_t count);
+/* HBM budget (bytes) of the resident cases plus the unreleased results (admission control). */
+int ufvm_service_set_memory_budget(ufvm_service* s, int64_t bytes);
 /* Tickets that finished (converged, stopped or failed) since the previous poll, oldest first:
  * writes min(capacity, pending) of them and their count; the rest stay for the next poll. */
 int ufvm_service_poll(ufvm_service* s, int64_t* tickets, int64_t capacity, int64_t* n_out);
@@ -263,8 +287,13 @@ int ufvm_service_stream(ufvm_service* s, void** stream);
  * current resident batch, reps times, and returns the average device time (ms) of one unit and
  * its compulsory DRAM bytes. kernel 0: one symmetric FP64 multicolour Gauss-Seidel sweep of
  * every case's level 0 (the U smoother); 1: the same sweep in FP32 on the V-cycle's level 0;
- * 2: the FP64 product q = A p of the flexible CG. The sweeps overwrite the correction vectors,
- * which the next step's assembly resets, so call it between steps. */
+ * 2: the FP64 product q = A p of the flexible CG; 3: the momentum assembly of one component;
+ * 4: the pressure-correction assembly (Rhie-Chow face flux and the p matrix); 5: the field
+ * update (boundary values, Gauss gradients of U and p); 6: one pass of the per-case coarse
+ * V-cycle kernel (latency-bound). The sweeps overwrite the correction vectors, which the next
+ * step's assembly resets, so call it between steps; kernels 3-5 recompute matrices and fields
+ * from the current state (4 also advances the face mass flux): use them on a batch kept only
+ * for timing. */
 int ufvm_service_profile(ufvm_service* s, int32_t kernel, int32_t reps, double* ms_per_unit,
                          double* bytes_per_unit);
 int ufvm_service_destroy(ufvm_service* s);

@@ -190,6 +190,7 @@ struct Case {
   WorkLists wl;
   int nsm = 148;
   int last_amg_cycles = 0;
+  long long dev_bytes = 0;  // device memory this case holds (the service's admission accounting)
 
   MeshView mv() const;
   FieldView fv();

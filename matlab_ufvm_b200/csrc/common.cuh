@@ -48,6 +48,11 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
   return (a0 * b0 + a1 * b1) + a2 * b2;
 }
 
+// Bytes of device memory this host thread holds through dalloc (freed by dfree). The batched
+// service takes differences of it around each case's allocations to learn the case's HBM
+// footprint.
+inline thread_local long long t_dev_bytes = 0;
+
 // Device array owned by a case; freed by its owner.
 template <typename T>
 struct DArr {
@@ -58,21 +63,30 @@ struct DArr {
 template <typename T>
 int dalloc(DArr<T>& a, size_t n) {
   if (a.p && a.n >= n) return UFVM_OK;
-  if (a.p) cudaFree(a.p);
+  if (a.p) {
+    cudaFree(a.p);
+    t_dev_bytes -= (long long)(a.n * sizeof(T));
+  }
   a.p = nullptr;
   a.n = 0;
   if (n == 0) n = 1;
   cudaError_t e = cudaMalloc((void**)&a.p, n * sizeof(T));
   if (e != cudaSuccess) {
+    a.p = nullptr;
+    cudaGetLastError();  // an out-of-memory report is not sticky: clear it for later checks
     set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
     return UFVM_E_OOM;
   }
   a.n = n;
+  t_dev_bytes += (long long)(n * sizeof(T));
   return UFVM_OK;
 }
 template <typename T>
 void dfree(DArr<T>& a) {
-  if (a.p) cudaFree(a.p);
+  if (a.p) {
+    cudaFree(a.p);
+    t_dev_bytes -= (long long)(a.n * sizeof(T));
+  }
   a.p = nullptr;
   a.n = 0;
 }

@@ -891,6 +891,8 @@ int Service::rebuild_tables() {
   }
   UFVM_CHECK(upload_vec(dcoarsest, hco, stream));
   UFVM_CHECK(upload_vec(dgstart, hg, stream));
+  h_coarsest = hco;
+  h_gstart = hg;
   {  // CTA order of the coarse V-cycle: the cases with the most rows below the grid levels first
     std::vector<long long> work_rows(ns, 0);
     for (int q = 0; q < ns; ++q)
@@ -1059,6 +1061,13 @@ BatchLaunch Service::batch() {
 
 // The reference's agglomeration of the assembled p matrix, FP32 arrays and colourings.
 int Service::ensure_hierarchy(Case& c) {
+  const long long b0 = t_dev_bytes;
+  const int st = ensure_hierarchy_(c);
+  c.dev_bytes += t_dev_bytes - b0;
+  return st;
+}
+
+int Service::ensure_hierarchy_(Case& c) {
   c.amg->smoother = UFVM_SMOOTHER_MCGS; c.amg->quirks = c.S.quirks;
   UFVM_CHECK(c.amg->build(c.lev, c.S.p_max_coarse_levels, c.S.quirks, &c.n_levels));
   for (int l = 0; l < c.n_levels; ++l) {
@@ -1509,8 +1518,10 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
   conv.assign(ns, 0);
   if (ns == 0) return UFVM_OK;
   for (auto* c : cases) {
+    const long long b0 = t_dev_bytes;
     if (c->lev.empty() || !c->lev[0].rowptr.p) UFVM_CHECK(c->fresh_level0());
     if (!c->lev[0].color_valid) { UFVM_CHECK(build_coloring(c->lin, c->lev[0])); tables_dirty = true; }
+    c->dev_bytes += t_dev_bytes - b0;
   }
   if (tables_dirty) UFVM_CHECK(rebuild_tables());
   ++n_iter_calls;
@@ -1609,8 +1620,24 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
 //      once -- + 12 B per nonzero);
 //   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32, colour-permuted ELL):
 //      2 x (16 B per row -- ac, bc, x written, x read once -- + 8 B per nonzero);
-//   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz.
-// The sweeps overwrite the slots' correction vectors, which the next assembly re-zeroes.
+//   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz;
+//   3: the momentum assembly of one component (k_uface, k_assemble_u, k_du_boundary and the
+//      residual reduction): per cell 8 phi + 24 grad phi + 16 (ac, bc), per interior face
+//      8 index + 8 mdot + 8 gamma + 8 gDiff + 24 T + 8 gf + 16 (two off-diagonals) bytes;
+//   4: the pressure-correction assembly (k_rhiechow, k_assemble_p and the mass-imbalance
+//      reduction): per cell 8 p + 24 grad p + 24 U + 24 DU + 16 (ac, bc), per interior face
+//      8 index + 8 gf + 24 Sf + 24 eCF + 8 |CF| + 8 mdot old + 8 mdot new + 16 (C1, C2) +
+//      16 (two off-diagonals) bytes;
+//   5: the field update (boundary values, the Gauss gradients of U and p with their boundary
+//      fixes, the velocity scale): over the Nc + Fb rows R, per U component 8 read + 24 gradient
+//      written, 8 + 24 for p; per face 24 Sf, per interior face 8 index + 8 gf, per cell 8 V
+//      for each of the two gradients;
+//   6: one pass of the packed coarse V-cycle kernel (k_coarse_vcycle_pk) over every slot's
+//      levels below its grid levels: latency-bound; bytes counted as five passes (a symmetric
+//      pre- and post-sweep, the residual) over each such level's 16 B per row + 8 B per nonzero.
+// The sweeps overwrite the slots' correction vectors, which the next assembly re-zeroes; units
+// 3-5 rewrite matrices and fields from the current state (unit 4 also advances the face mass
+// flux), so a batch profiled with them is only fit for timing.
 int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   const int ns = (int)cases.size();
   if (ns == 0 || reps <= 0) { set_error("profile: no resident case or reps <= 0"); return UFVM_E_INVALID; }
@@ -1636,16 +1663,29 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
           if (l0_items) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(wsm0.p + smoff[0][c], pctl.p);
           else k_mc32<<<smcnt[0][c], kBlock, 0, stream>>>(levTab.p, ns, 0, wsm[0].p + smoff[0][c], c, pctl.p);
         }
-    } else {
+    } else if (kernel == 2) {
       k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p,
                                           reinterpret_cast<double2*>(fcg.p + (((size_t)nwc + 1) & ~(size_t)1) +
                                                                      (((size_t)ns + 1) & ~(size_t)1)));
+    } else if (kernel == 3) {
+      UFVM_CHECK(stage_assemble_u(batch(), 0));
+    } else if (kernel == 4) {
+      UFVM_CHECK(stage_assemble_p(batch()));
+    } else if (kernel == 5) {
+      UFVM_CHECK(stage_update_fields(batch()));
+    } else {
+      if (use_packing && npk_tasks > 0)
+        k_coarse_vcycle_pk<<<npk_tasks, kBlockPack, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p,
+                                                                S.p_pre_sweep, S.p_post_sweep, pctl.p, dpk_tasks.p);
+      else
+        k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, S.p_pre_sweep,
+                                                 S.p_post_sweep, pctl.p, dcta_order.p);
     }
     UFVM_LAUNCH_CHECK();
     return UFVM_OK;
   };
-  if (kernel < 0 || kernel > 2) { set_error("profile: unknown kernel id"); return UFVM_E_INVALID; }
-  if (kernel >= 1) {
+  if (kernel < 0 || kernel > 6) { set_error("profile: unknown kernel id"); return UFVM_E_INVALID; }
+  if (kernel == 1 || kernel == 2 || kernel == 6) {
     for (auto* c : cases)
       if (!c->hierarchy_valid) { set_error("profile: a resident case has no AMG hierarchy yet"); return UFVM_E_INVALID; }
     if (Lmax < 2 || nwsm.empty()) { set_error("profile: no AMG hierarchy yet"); return UFVM_E_INVALID; }
@@ -1670,9 +1710,21 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   *ms = t / reps;
+  double Fi = 0, F = 0, R = 0;
+  for (auto* c : cases) { Fi += c->M.Fi; F += c->M.F; R += c->M.Nc + c->M.Fb; }
   if (kernel == 0) *bytes = 2.0 * (32.0 * N + 12.0 * NNZ);
   else if (kernel == 1) *bytes = 2.0 * (16.0 * N + 8.0 * NNZ);
-  else *bytes = 36.0 * N + 12.0 * NNZ;
+  else if (kernel == 2) *bytes = 36.0 * N + 12.0 * NNZ;
+  else if (kernel == 3) *bytes = 48.0 * N + 80.0 * Fi;
+  else if (kernel == 4) *bytes = 96.0 * N + 120.0 * Fi;
+  else if (kernel == 5) *bytes = (3 * 32.0 + 32.0) * R + 2 * (24.0 * F + 16.0 * Fi + 8.0 * N);
+  else {
+    double b = 0;
+    for (int q = 0; q < ns && q < (int)h_gstart.size(); ++q)
+      for (int l = h_gstart[q]; l <= h_coarsest[q] && l < cases[q]->n_levels; ++l)
+        b += 5.0 * (16.0 * cases[q]->lev[l].n + 8.0 * cases[q]->lev[l].nnz);
+    *bytes = b;
+  }
   return UFVM_OK;
 }
 

@@ -91,6 +91,7 @@ struct Service {
   int maxg = 0;                      // max over slots of g
   DArr<int> dcoarsest;               // per slot: index of its coarsest level
   DArr<int> dgstart;                 // per slot: g
+  std::vector<int> h_gstart, h_coarsest;  // host copies of dgstart / dcoarsest
   DArr<int> dcta_order;              // slots in the CTA order of the coarse V-cycle (largest first)
   DArr<PackTask> dpk_tasks;          // packed tasks of the coarse V-cycle
   std::vector<unsigned char> vel_mask;  // boundary-velocity correction launches with work
@@ -143,7 +144,8 @@ struct Service {
   int rebuild_tables();
   BatchLaunch batch();
   bool needs_hierarchy(const Case& c) const;
-  int ensure_hierarchy(Case& c);
+  int ensure_hierarchy(Case& c);   // adds the bytes it allocates to c.dev_bytes
+  int ensure_hierarchy_(Case& c);
   int build_ell(Case& c);
   int loop_begin(int kind, cudaGraphConditionalHandle* h);
   int loop_end();

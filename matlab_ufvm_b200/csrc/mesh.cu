@@ -116,20 +116,35 @@ __global__ void k_face_geometry2(int F, int Fi, const int* __restrict__ owner, c
 }
 
 // Sum over a noSlip patch of n_c^2 for c = 0..2, sequential in face order (the value
-// MATLAB's dot() of two row vectors returns, cfdAssembleDiffusionTerm.m:535,541,547).
-__global__ void k_patch_nsum(int nPatch, const int* __restrict__ pstart, const int* __restrict__ pn,
-                             const double* __restrict__ Sx, const double* __restrict__ Sy,
-                             const double* __restrict__ Sz, const double* __restrict__ area, double* out) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nPatch) return;
-  double s0 = 0, s1 = 0, s2 = 0;
-  for (int j = 0; j < pn[p]; ++j) {
-    const int f = pstart[p] + j;
-    const double A = area[f];
-    const double n0 = Sx[f] / A, n1 = Sy[f] / A, n2 = Sz[f] / A;
-    s0 = s0 + n0 * n0; s1 = s1 + n1 * n1; s2 = s2 + n2 * n2;
+// MATLAB's dot() of two row vectors returns, cfdAssembleDiffusionTerm.m:535,541,547). One block
+// per patch: the block stages a chunk of the patch's faces through shared memory with coalesced
+// loads and forms the squares in parallel; threads 0..2 then add one component each in face
+// order, so each sum is the same chain of additions as the sequential loop.
+constexpr int kNsumChunk = 256;
+__global__ void __launch_bounds__(kNsumChunk) k_patch_nsum(const int* __restrict__ pstart, const int* __restrict__ pn,
+                                                           const double* __restrict__ Sx, const double* __restrict__ Sy,
+                                                           const double* __restrict__ Sz,
+                                                           const double* __restrict__ area, double* out) {
+  __shared__ double sq[3][kNsumChunk];
+  const int p = blockIdx.x, t = threadIdx.x;
+  const int n = pn[p], f0 = pstart[p];
+  double s = 0;
+  for (int base = 0; base < n; base += kNsumChunk) {
+    const int j = base + t;
+    if (j < n) {
+      const int f = f0 + j;
+      const double A = area[f];
+      const double n0 = Sx[f] / A, n1 = Sy[f] / A, n2 = Sz[f] / A;
+      sq[0][t] = n0 * n0; sq[1][t] = n1 * n1; sq[2][t] = n2 * n2;
+    }
+    __syncthreads();
+    if (t < 3) {
+      const int cnt = min(kNsumChunk, n - base);
+      for (int k = 0; k < cnt; ++k) s = s + sq[t][k];
+    }
+    __syncthreads();
   }
-  out[3 * p] = s0; out[3 * p + 1] = s1; out[3 * p + 2] = s2;
+  if (t < 3) out[3 * p + t] = s;
 }
 
 int Case::build_mesh(const ufvm_mesh_desc* d) {
@@ -208,9 +223,12 @@ int Case::build_mesh(const ufvm_mesh_desc* d) {
                                                       M.Tx.p, M.Ty.p, M.Tz.p, M.gf.p, M.wd.p);
   UFVM_LAUNCH_CHECK();
   UFVM_CHECK(dalloc(D.pnsum, 3 * std::max(P.n, 1)));
-  k_patch_nsum<<<nblocks(P.n), kBlock, 0, stream>>>(P.n, D.pstart.p, D.pcount.p, M.Sx.p, M.Sy.p, M.Sz.p, M.area.p,
-                                                    D.pnsum.p);
-  UFVM_LAUNCH_CHECK();
+  if ((S.quirks & UFVM_Q14_NOSLIP_PATCH_SUM) && P.n > 0) {  // only the reference's patch-wide sum reads it
+    k_patch_nsum<<<P.n, kNsumChunk, 0, stream>>>(D.pstart.p, D.pcount.p, M.Sx.p, M.Sy.p, M.Sz.p, M.area.p, D.pnsum.p);
+    UFVM_LAUNCH_CHECK();
+  } else {
+    UFVM_CUDA(cudaMemsetAsync(D.pnsum.p, 0, 3 * std::max(P.n, 1) * sizeof(double), stream));
+  }
   UFVM_CUDA(cudaStreamSynchronize(stream));
   dfree(pts); dfree(fstart); dfree(fnodes);
   return UFVM_OK;

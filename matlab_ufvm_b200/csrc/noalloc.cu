@@ -17,6 +17,10 @@
 //     previous call left in it; each call clears the parts that must start at zero. Calls whose
 //     device work overlaps (different streams, or different host threads) race on the scratch
 //     and give wrong results: serialise them;
+//   * the matrix must be structurally symmetric (a face couples both of its cells, so every
+//     finite-volume matrix is): the dependency levels come from each row's lower neighbours,
+//     which orders the sweep correctly only when a row's upper neighbours list it in turn;
+//     ufvm_solve_sor makes the same assumption;
 //   * the first call on a device looks up the scratch array's device address with
 //     cudaGetSymbolAddress (with that device current) and caches it; make that first call
 //     before any stream capture that might include this function.

@@ -1,10 +1,18 @@
 // service_api.cu -- extern "C" entry points of the batched steady-case service.
 //
-// Admission policy: first come, first served, while the sum of resident cells stays within
-// max_resident_cells; a case that alone exceeds the budget is admitted when the service is
-// empty. Each ufvm_service_step advances every resident case by one SIMPLE iteration
-// (fast.cu), then retires finished cases and admits queued ones, so requests that arrive
-// while others run join the batch as soon as cells free up (continuous batching).
+// Admission policy: first come, first served, while the estimated HBM footprint of the resident
+// cases stays within the memory budget (and the sum of resident cells within max_resident_cells);
+// a case that alone exceeds the budget is admitted when the service is empty. Each
+// ufvm_service_step advances every resident case by one SIMPLE iteration (fast.cu), then retires
+// finished cases and admits queued ones, so requests that arrive while others run join the batch
+// as soon as memory frees up (continuous batching).
+//
+// A finished case keeps its slot in the batch, frozen, until the slots are next rebuilt: its
+// result (U, p, mdot at the finishing iteration) is copied to a snapshot on the device, and the
+// case may run a few more iterations that nobody reads. Rebuilding the slot tables re-captures the
+// tick's CUDA graph, so departures are gathered: the frozen slots are dropped when queued cases
+// are admitted, when their cells pass 1/16 of the active cells, when one has waited 32 steps, or
+// when no active case is left.
 #include <deque>
 #include <map>
 #include <memory>
@@ -20,6 +28,14 @@ struct Pending {
   std::vector<double> points, bvu, bvp;
   std::vector<int32_t> fs, fn, own, nei, ptype, pstart, pn, bcu, bcp;
   double t_submit;  // service clock (ms) at submission
+  long long cells = 0, est_raw = 0;
+};
+
+// Result of a finished case, copied on the device when it finished.
+struct Snapshot {
+  double *U = nullptr, *p = nullptr, *mdot = nullptr;
+  size_t nU = 0, np = 0, nm = 0;
+  long long bytes() const { return (long long)((nU + np + nm) * sizeof(double)); }
 };
 
 struct Record {
@@ -28,16 +44,27 @@ struct Record {
   int iterations = 0, max_iter = 0;
   double res[16] = {0};
   double t_submit = 0, t_admit = 0, t_done = 0;
-  Case* c = nullptr;  // owned while resident or finished-unreleased
-  long long cells = 0;
-  std::string err;    // why admission or a step failed
+  Case* c = nullptr;  // the case while it holds a slot; after that only if it has no snapshot
+  Snapshot snap;
+  long long cells = 0, est_raw = 0;
+  bool released = false;  // released while its slot was still frozen in the batch
+  std::string err;        // why admission or a step failed
 };
 
 struct ServiceImpl {
   Service svc;
   long long max_cells = 0, resident_cells = 0, next_ticket = 1, finished = 0;
+  // HBM budget of the resident cases (their measured allocations, or the estimate of a case whose
+  // hierarchy is not built yet) and of the snapshots of finished, unreleased results
+  long long max_bytes = 0, snap_bytes = 0;
+  double est_scale = 1.0;  // largest measured footprint / estimate seen so far (>= 1)
+  long long n_deferred_mem = 0, n_oom_requeue = 0, n_drops = 0;
   std::deque<Pending> queue;
   std::map<long long, Record> rec;
+  std::vector<char> frozen;     // per slot of svc.cases: finished, result in its snapshot
+  std::vector<int> frozen_age;  // steps since the slot froze
+  bool force_drop = false;
+  std::map<long long, int> inject_oom;  // fault injection: admissions of a ticket that fail as OOM
   double clock_ms = 0;  // accumulated device time of all steps
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   // admission runs at most every admit_interval steps unless the resident cells fall to half
@@ -57,32 +84,106 @@ struct ServiceImpl {
   std::vector<int> tune_n;
   std::vector<long long> finished_unpolled;  // tickets finished since the last poll
   ~ServiceImpl() {
-    for (auto& kv : rec)
-      if (kv.second.c && kv.second.state >= 2) { delete kv.second.c; kv.second.c = nullptr; }
+    for (auto& kv : rec) {
+      // ufvm_service_destroy has cleared the cases that hold slots (the Service frees those)
+      if (kv.second.c) delete kv.second.c;
+      kv.second.c = nullptr;
+      free_snapshot(kv.second.snap);
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
   }
+  static void free_snapshot(Snapshot& s) {
+    for (double** q : {&s.U, &s.p, &s.mdot})
+      if (*q) { cudaFree(*q); *q = nullptr; }
+    s.nU = s.np = s.nm = 0;
+  }
+  long long active_cells() const { return resident_cells; }
+  long long slot_bytes() const {
+    long long b = 0;
+    for (size_t q = 0; q < svc.cases.size(); ++q) {
+      const Record& r = rec.at(svc.tickets[q]);
+      // before its first iteration a case holds no hierarchy yet: count the estimate
+      b += std::max<long long>(svc.cases[q]->dev_bytes, r.iterations == 0 ? estimate(r.est_raw) : 0);
+    }
+    return b;
+  }
+  long long estimate(long long raw) const { return (long long)(1.05 * est_scale * (double)raw); }
 };
 
+// Device bytes of a case before its hierarchy, from its sizes: the mesh geometry (23 face and
+// cell arrays), the fields over cells and boundary rows (U, its gradient, p, the p and PP
+// gradients, DU: 23 rows of doubles), the per-face momentum terms and fluxes, the level-0 matrix,
+// its schedules and colour-major copies, and the agglomeration hierarchy with its FP32 and ELL
+// copies (about as much again as the level-0 matrix). The service scales it by the largest
+// ratio of measured to estimated bytes it has seen.
+static long long estimate_raw(long long Nc, long long F, long long Fi, long long nodes) {
+  const long long Fb = F - Fi, R = Nc + Fb, nnz = 2 * Fi;
+  const long long dbl = 19 * F + 4 * Nc + 23 * R + 10 * F + 8 * Nc + 2 * (nnz + 8 * Nc) + 4 * nnz;
+  const long long ints = 3 * F + 4 * Fi + 6 * Nc + 3 * nnz + nodes / 4;
+  return 8 * dbl + 4 * ints;
+}
+
+static void fill_desc(const Pending& p, ufvm_mesh_desc& d) {
+  d.n_points = (int32_t)(p.points.size() / 3); d.points = p.points.data();
+  d.n_faces = (int32_t)p.own.size(); d.face_start = p.fs.data(); d.face_nodes = p.fn.data();
+  d.n_interior = (int32_t)p.nei.size(); d.owner = p.own.data(); d.neighbour = p.nei.data();
+  d.n_patches = (int32_t)p.ptype.size(); d.patch_type = p.ptype.data(); d.patch_start = p.pstart.data();
+  d.patch_n = p.pn.data();
+}
+
+// Finished slots leave the batch: each case's memory is freed (its result lives in its
+// snapshot) and the slot tables are rebuilt at the next iteration.
+static void drop_frozen(ServiceImpl& S) {
+  Service& V = S.svc;
+  std::vector<Case*> keep;
+  std::vector<long long> keept;
+  std::vector<char> kf;
+  std::vector<int> ka;
+  bool any = false;
+  for (size_t q = 0; q < V.cases.size(); ++q) {
+    if (!S.frozen[q]) {
+      keep.push_back(V.cases[q]); keept.push_back(V.tickets[q]); kf.push_back(0); ka.push_back(S.frozen_age[q]);
+      continue;
+    }
+    any = true;
+    auto it = S.rec.find(V.tickets[q]);
+    Record& r = it->second;
+    if (r.released) {  // nobody will read it: free the case and forget the ticket
+      delete V.cases[q];
+      S.rec.erase(it);
+    } else if (r.snap.U) {  // the snapshot holds the result: free the case
+      delete V.cases[q];
+      r.c = nullptr;
+    }  // else the record keeps the case (its fields are the result)
+  }
+  if (!any) return;
+  V.cases = keep; V.tickets = keept; S.frozen = kf; S.frozen_age = ka;
+  V.tables_dirty = true;
+  ++S.n_drops;
+  S.force_drop = false;
+}
+
+static bool admission_due(const ServiceImpl& S) {
+  if (S.queue.empty()) return false;
+  return S.resident_cells == 0 || S.steps_since_admit >= S.admit_interval || 2 * S.resident_cells <= S.max_cells;
+}
+
 static int admit(ServiceImpl& S) {
-  if (S.queue.empty()) return UFVM_OK;
-  if (!S.svc.cases.empty() && S.steps_since_admit < S.admit_interval && 2 * S.resident_cells > S.max_cells)
-    return UFVM_OK;
+  if (!admission_due(S)) return UFVM_OK;
+  drop_frozen(S);  // departures are gathered into the admission's table rebuild
   const size_t before = S.svc.cases.size();
   while (!S.queue.empty()) {
     Pending& p = S.queue.front();
-    const long long nc_est = (long long)(p.own.empty() ? 0 : 1);
-    long long ncell = 0;
-    for (int32_t o : p.own) ncell = std::max<long long>(ncell, o + 1);
-    for (int32_t o : p.nei) ncell = std::max<long long>(ncell, o + 1);
-    (void)nc_est;
-    if (!S.svc.cases.empty() && S.resident_cells + ncell > S.max_cells) break;
+    const long long est = S.estimate(p.est_raw);
+    if (!S.svc.cases.empty()) {
+      if (S.resident_cells + p.cells > S.max_cells) break;
+      if (S.slot_bytes() + S.snap_bytes + est > S.max_bytes) { ++S.n_deferred_mem; break; }
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (long long)fr < est + (est >> 3)) { ++S.n_deferred_mem; break; }
+    }
     ufvm_mesh_desc d;
-    d.n_points = (int32_t)(p.points.size() / 3); d.points = p.points.data();
-    d.n_faces = (int32_t)p.own.size(); d.face_start = p.fs.data(); d.face_nodes = p.fn.data();
-    d.n_interior = (int32_t)p.nei.size(); d.owner = p.own.data(); d.neighbour = p.nei.data();
-    d.n_patches = (int32_t)p.ptype.size(); d.patch_type = p.ptype.data(); d.patch_start = p.pstart.data();
-    d.patch_n = p.pn.data();
+    fill_desc(p, d);
     ufvm_settings cs = S.svc.S;
     cs.nu = p.nu;
     // the pressure reference cell is per case, as in cfdReadSystem.m:238-252: a case whose
@@ -93,9 +194,26 @@ static int admit(ServiceImpl& S) {
       if (t != UFVM_PATCH_WALL && t != UFVM_PATCH_EMPTY && t != UFVM_PATCH_SYMMETRY) closed = false;
     cs.fixed_element = closed ? std::max(0, S.svc.S.fixed_element) : -1;
     Case* c = new Case();
-    const int st = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr,
-                                    nullptr, nullptr, S.svc.stream);
+    const long long b0 = t_dev_bytes;
+    int st;
+    auto inj = S.inject_oom.find(p.ticket);
+    if (inj != S.inject_oom.end() && inj->second > 0) {  // a failed device allocation, injected
+      --inj->second;
+      set_error("cudaMalloc: out of memory (injected)");
+      st = UFVM_E_OOM;
+    } else {
+      st = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr, nullptr,
+                            nullptr, S.svc.stream);
+    }
+    c->dev_bytes = t_dev_bytes - b0;
     Record& r = S.rec[p.ticket];
+    if (st == UFVM_E_OOM && !S.svc.cases.empty()) {
+      // the device is full after all: the request waits at the head of the queue for memory
+      delete c;
+      cudaGetLastError();
+      ++S.n_oom_requeue;
+      break;
+    }
     r.t_admit = S.clock_ms;
     if (st != UFVM_OK) {
       r.err = get_error();
@@ -110,15 +228,53 @@ static int admit(ServiceImpl& S) {
     }
     r.state = 1;
     r.c = c;
-    r.cells = ncell;
-    S.resident_cells += ncell;
+    r.cells = p.cells;
+    r.est_raw = p.est_raw;
+    S.resident_cells += p.cells;
     S.svc.cases.push_back(c);
     S.svc.tickets.push_back(p.ticket);
+    S.frozen.push_back(0);
+    S.frozen_age.push_back(0);
     S.svc.tables_dirty = true;
     S.queue.pop_front();
   }
   if (S.svc.cases.size() != before) S.steps_since_admit = 0;
   return UFVM_OK;
+}
+
+// Copies a finishing case's result to a device snapshot (stream-ordered allocations, no device
+// synchronisation). Returns false when there is no memory for it: the slot then leaves the batch
+// at once and the record keeps the case itself.
+static bool snapshot(ServiceImpl& S, Record& r, Case& C) {
+  Snapshot& s = r.snap;
+  const size_t R = C.M.Nc + C.M.Fb;
+  s.nU = 3 * (size_t)C.rowsU; s.np = R; s.nm = (size_t)C.M.F;
+  cudaStream_t st = S.svc.stream;
+  if (cudaMallocAsync((void**)&s.U, s.nU * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync((void**)&s.p, s.np * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync((void**)&s.mdot, s.nm * sizeof(double), st) != cudaSuccess) {
+    cudaGetLastError();
+    for (double** q : {&s.U, &s.p, &s.mdot})
+      if (*q) { cudaFreeAsync(*q, st); *q = nullptr; }
+    s.nU = s.np = s.nm = 0;
+    return false;
+  }
+  bool ok = true;
+  for (int c = 0; c < 3; ++c)
+    ok = ok && cudaMemcpyAsync(s.U + (size_t)c * C.rowsU, C.U[c].p, (size_t)C.rowsU * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(s.p, C.p.p, R * sizeof(double), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(s.mdot, C.mdot.p, (size_t)C.M.F * sizeof(double), cudaMemcpyDeviceToDevice, st) ==
+                 cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    for (double** q : {&s.U, &s.p, &s.mdot})
+      if (*q) { cudaFreeAsync(*q, st); *q = nullptr; }
+    s.nU = s.np = s.nm = 0;
+    return false;
+  }
+  S.snap_bytes += s.bytes();
+  return true;
 }
 
 // One step of the schedule autotuner (called after every timed step).
@@ -193,6 +349,10 @@ int ufvm_service_create(const ufvm_settings* settings, int64_t max_resident_cell
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&S.svc.nsm, cudaDevAttrMultiProcessorCount, dev);
   S.svc.lin.stream = S.svc.stream;
+  // default HBM budget: 90% of the device memory free when the service starts
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
+  S.max_bytes = (long long)(0.9 * (double)fr);
   *out = h;
   return UFVM_OK;
 }
@@ -223,6 +383,9 @@ int ufvm_service_submit(ufvm_service* h, const ufvm_mesh_desc* m, double nu, con
   p.bvu.assign(bc_val_u, bc_val_u + 3 * (size_t)Fb);
   p.bvp.assign(bc_val_p, bc_val_p + Fb);
   p.t_submit = S.clock_ms;
+  for (int32_t o : p.own) p.cells = std::max<long long>(p.cells, (long long)o + 1);
+  for (int32_t o : p.nei) p.cells = std::max<long long>(p.cells, (long long)o + 1);
+  p.est_raw = estimate_raw(p.cells, F, m->n_interior, (long long)p.fn.size());
   Record& r = S.rec[p.ticket];
   r.state = 0;
   r.max_iter = max_iter;
@@ -236,6 +399,21 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
   if (!h) return UFVM_E_INVALID;
   ServiceImpl& S = h->impl;
   Service& V = S.svc;
+  {
+    // gather departures: drop the frozen slots when they hold a sixteenth of the active cells,
+    // when one has waited 32 steps, when no active case is left, or after a failure
+    long long fcells = 0;
+    int oldest = 0;
+    bool anyf = false;
+    for (size_t q = 0; q < V.cases.size(); ++q)
+      if (S.frozen[q]) {
+        anyf = true;
+        fcells += S.rec[V.tickets[q]].cells;
+        oldest = std::max(oldest, S.frozen_age[q]);
+      }
+    if (anyf && (S.force_drop || 16 * fcells >= S.resident_cells || oldest >= 32 || S.resident_cells == 0))
+      drop_frozen(S);
+  }
   UFVM_CHECK(admit(S));
   ++S.steps;
   if (!V.cases.empty()) {
@@ -251,33 +429,33 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
     UFVM_CUDA(cudaEventElapsedTime(&ms, S.e0, S.e1));
     S.clock_ms += ms;
     tune_step(S, ms, V.n_graph_ticks != graph_before);
-    std::vector<Case*> keep;
-    std::vector<long long> keept;
     for (size_t q = 0; q < V.cases.size(); ++q) {
+      if (S.frozen[q]) { ++S.frozen_age[q]; continue; }
       Record& r = S.rec[V.tickets[q]];
       r.iterations += 1;
+      if (r.iterations == 1 && r.est_raw > 0)  // hierarchy built: learn the footprint estimate's error
+        S.est_scale = std::max(S.est_scale, (double)V.cases[q]->dev_bytes / (double)r.est_raw);
       std::copy(&res[q * 16], &res[q * 16] + 16, r.res);
       bool done = false;
       if (conv[q] == 1) { r.state = 2; r.status = UFVM_OK; done = true; }
-      else if (conv[q] < 0) { r.state = 3; r.status = -conv[q]; done = true; }
+      else if (conv[q] < 0) { r.state = 3; r.status = -conv[q]; done = true; S.force_drop = true; }
       else if (r.max_iter > 0 && r.iterations >= r.max_iter) { r.state = 3; r.status = UFVM_E_NOT_CONVERGED; done = true; }
       if (done) {
         r.t_done = S.clock_ms;
         S.resident_cells -= r.cells;
         ++S.finished;
         S.finished_unpolled.push_back(V.tickets[q]);
-        V.tables_dirty = true;
-      } else {
-        keep.push_back(V.cases[q]);
-        keept.push_back(V.tickets[q]);
+        S.frozen[q] = 1;
+        S.frozen_age[q] = 0;
+        if (!snapshot(S, r, *V.cases[q])) S.force_drop = true;  // no room: the case leaves at once
       }
     }
-    V.cases = keep;
-    V.tickets = keept;
   }
   ++S.steps_since_admit;
   UFVM_CHECK(admit(S));
-  if (n_resident) *n_resident = (int32_t)V.cases.size();
+  int active = 0;
+  for (char f : S.frozen) active += f ? 0 : 1;
+  if (n_resident) *n_resident = active;
   if (n_queued) *n_queued = (int32_t)S.queue.size();
   if (n_finished_total) *n_finished_total = S.finished;
   return UFVM_OK;
@@ -287,7 +465,7 @@ int ufvm_service_status(ufvm_service* h, int64_t ticket, int32_t* state, int32_t
                         double* res16, double* latency_ms, double* queue_ms) {
   if (!h) return UFVM_E_INVALID;
   auto it = h->impl.rec.find(ticket);
-  if (it == h->impl.rec.end()) { set_error("unknown ticket"); return UFVM_E_INVALID; }
+  if (it == h->impl.rec.end() || it->second.released) { set_error("unknown ticket"); return UFVM_E_INVALID; }
   const Record& r = it->second;
   if (state) *state = r.state;
   if (status) *status = r.status;
@@ -303,21 +481,29 @@ int ufvm_service_get_field(ufvm_service* h, int64_t ticket, const char* name, do
                            int64_t* written) {
   if (!h) return UFVM_E_INVALID;
   auto it = h->impl.rec.find(ticket);
-  if (it == h->impl.rec.end()) { set_error("unknown ticket"); return UFVM_E_INVALID; }
-  if (!it->second.c) {
+  if (it == h->impl.rec.end() || it->second.released) { set_error("unknown ticket"); return UFVM_E_INVALID; }
+  const Record& rc = it->second;
+  if (!rc.c && !rc.snap.U) {
     set_error("ticket has no resident or finished case" +
-              (it->second.err.empty() ? std::string() : " (admission failed: " + it->second.err + ")"));
+              (rc.err.empty() ? std::string() : " (admission failed: " + rc.err + ")"));
     return UFVM_E_INVALID;
   }
-  // borrow the case through a temporary handle-free path
-  Case& C = *it->second.c;
-  const size_t R = C.M.Nc + C.M.Fb;
   std::string s(name ? name : "");
   std::vector<std::pair<const double*, size_t>> src;
-  if (s == "U") { for (int c = 0; c < 3; ++c) src.push_back({C.U[c].p, (size_t)C.rowsU}); }
-  else if (s == "p") src.push_back({C.p.p, R});
-  else if (s == "mdot") src.push_back({C.mdot.p, (size_t)C.M.F});
-  else { set_error("unknown field " + s); return UFVM_E_INVALID; }
+  cudaStream_t stream = h->impl.svc.stream;
+  if (rc.snap.U) {  // a finished case: its result as of the iteration it finished
+    if (s == "U") src.push_back({rc.snap.U, rc.snap.nU});
+    else if (s == "p") src.push_back({rc.snap.p, rc.snap.np});
+    else if (s == "mdot") src.push_back({rc.snap.mdot, rc.snap.nm});
+    else { set_error("unknown field " + s); return UFVM_E_INVALID; }
+  } else {
+    Case& C = *rc.c;
+    const size_t R = C.M.Nc + C.M.Fb;
+    if (s == "U") { for (int c = 0; c < 3; ++c) src.push_back({C.U[c].p, (size_t)C.rowsU}); }
+    else if (s == "p") src.push_back({C.p.p, R});
+    else if (s == "mdot") src.push_back({C.mdot.p, (size_t)C.M.F});
+    else { set_error("unknown field " + s); return UFVM_E_INVALID; }
+  }
   size_t tot = 0;
   for (auto& x : src) tot += x.second;
   if (written) *written = (int64_t)tot;
@@ -325,10 +511,10 @@ int ufvm_service_get_field(ufvm_service* h, int64_t ticket, const char* name, do
   if ((int64_t)tot > n) { set_error("host buffer too small"); return UFVM_E_INVALID; }
   size_t off = 0;
   for (auto& x : src) {
-    UFVM_CUDA(cudaMemcpyAsync(host + off, x.first, x.second * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    UFVM_CUDA(cudaMemcpyAsync(host + off, x.first, x.second * sizeof(double), cudaMemcpyDeviceToHost, stream));
     off += x.second;
   }
-  UFVM_CUDA(cudaStreamSynchronize(C.stream));
+  UFVM_CUDA(cudaStreamSynchronize(stream));
   return UFVM_OK;
 }
 
@@ -337,8 +523,24 @@ int ufvm_service_release(ufvm_service* h, int64_t ticket) {
   auto it = h->impl.rec.find(ticket);
   if (it == h->impl.rec.end()) return UFVM_OK;
   if (it->second.state == 1) { set_error("ticket is still resident"); return UFVM_E_INVALID; }
-  if (it->second.c) { delete it->second.c; it->second.c = nullptr; }
-  h->impl.rec.erase(it);
+  Record& r = it->second;
+  if (r.released) { set_error("unknown ticket"); return UFVM_E_INVALID; }
+  ServiceImpl& S = h->impl;
+  if (r.snap.U) {
+    S.snap_bytes -= r.snap.bytes();
+    for (double** q : {&r.snap.U, &r.snap.p, &r.snap.mdot})
+      if (*q) { cudaFreeAsync(*q, S.svc.stream); *q = nullptr; }
+    r.snap.nU = r.snap.np = r.snap.nm = 0;
+  }
+  bool in_slot = false;
+  for (Case* c : S.svc.cases) in_slot = in_slot || (r.c && c == r.c);
+  if (in_slot) {  // still a frozen slot: it leaves the batch with the next departures
+    r.released = true;
+    return UFVM_OK;
+  }
+  if (r.c) delete r.c;  // a case without a snapshot belongs to its record
+  r.c = nullptr;
+  S.rec.erase(it);
   return UFVM_OK;
 }
 
@@ -355,6 +557,14 @@ int ufvm_service_stats(ufvm_service* h, double* out, int n) {
   v.push_back((double)V.launches_total);
   v.push_back((double)V.cta_rows);
   v.push_back((double)V.n_tunes);
+  v.push_back((double)(h->impl.slot_bytes() + h->impl.snap_bytes));
+  v.push_back((double)h->impl.max_bytes);
+  v.push_back((double)h->impl.n_deferred_mem);
+  v.push_back((double)h->impl.n_oom_requeue);
+  v.push_back((double)h->impl.n_drops);
+  v.push_back(h->impl.est_scale);
+  v.push_back((double)V.loops_seen[0]);  // U smoother loop bodies run by replayed ticks
+  v.push_back((double)V.loops_seen[1]);  // p V-cycle loop bodies run by replayed ticks
   for (int i = 0; i < n; ++i) out[i] = i < (int)v.size() ? v[i] : 0.0;
   return UFVM_OK;
 }
@@ -372,6 +582,29 @@ int ufvm_service_poll(ufvm_service* h, int64_t* tickets, int64_t capacity, int64
   for (int64_t i = 0; i < n; ++i) tickets[i] = f[i];
   f.erase(f.begin(), f.begin() + n);
   *n_out = n;
+  return UFVM_OK;
+}
+
+int ufvm_service_admit(ufvm_service* h, int32_t* n_resident) {
+  if (!h) return UFVM_E_INVALID;
+  ServiceImpl& S = h->impl;
+  S.steps_since_admit = 1 << 30;  // due now
+  UFVM_CHECK(admit(S));
+  int active = 0;
+  for (char f : S.frozen) active += f ? 0 : 1;
+  if (n_resident) *n_resident = active;
+  return UFVM_OK;
+}
+
+int ufvm_service_inject_admit_oom(ufvm_service* h, int64_t ticket, int32_t count) {
+  if (!h || count < 0) return UFVM_E_INVALID;
+  h->impl.inject_oom[ticket] = count;
+  return UFVM_OK;
+}
+
+int ufvm_service_set_memory_budget(ufvm_service* h, int64_t bytes) {
+  if (!h || bytes <= 0) { set_error("the memory budget must be positive"); return UFVM_E_INVALID; }
+  h->impl.max_bytes = bytes;
   return UFVM_OK;
 }
 
@@ -409,9 +642,10 @@ int ufvm_service_stream(ufvm_service* h, void** stream) {
 
 int ufvm_service_destroy(ufvm_service* h) {
   if (!h) return UFVM_OK;
-  // resident cases are owned by the Service; finished ones by their records
+  // cases in slots (active or frozen) are owned by the Service; the rest by their records
   for (auto& kv : h->impl.rec)
-    if (kv.second.state == 1) kv.second.c = nullptr;
+    for (Case* c : h->impl.svc.cases)
+      if (kv.second.c == c) kv.second.c = nullptr;
   delete h;
   return UFVM_OK;
 }

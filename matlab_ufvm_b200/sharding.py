@@ -1,9 +1,12 @@
 """Case sharding across GPUs: one process per GPU, independent cases, no data-path collective.
 
-Case i of a stream goes to rank i mod world_size. The only collectives are the ones that
-combine measurements: the sum of converged cases, the max over ranks of the timed duration,
-and the gathered per-case latencies. They run on any torch.distributed backend (NCCL with
-CUDA tensors on GPUs, gloo with CPU tensors in the tests).
+Two ways to hand cases to ranks. A batch workload (the 512-case sweep) is weakly scaled: rank r
+solves its own full batch, drawn from the same distribution with seed base + r, so the work per
+GPU is fixed as GPUs are added. A stream of requests is split: case i goes to rank
+i mod world_size. The only collectives are the ones that combine measurements: the sum of
+converged cases, the max over ranks of the timed duration, and the gathered per-case latencies.
+They run on any torch.distributed backend (NCCL with CUDA tensors on GPUs, gloo with CPU
+tensors in the tests).
 """
 from __future__ import annotations
 
@@ -15,6 +18,13 @@ def stream_index(rank: int, world_size: int, k: int) -> int:
     if not 0 <= rank < world_size:
         raise ValueError(f"rank {rank} outside world of {world_size}")
     return rank + world_size * k
+
+
+def batch_seed(rank: int, world_size: int, base: int) -> int:
+    """Seed of rank `rank`'s own batch under weak scaling (rank 0 keeps the base seed)."""
+    if not 0 <= rank < world_size:
+        raise ValueError(f"rank {rank} outside world of {world_size}")
+    return base + rank
 
 
 def shard(rank: int, world_size: int, n_total: int) -> List[int]:

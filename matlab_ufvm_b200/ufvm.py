@@ -396,6 +396,9 @@ def _service_lib():
         L.ufvm_service_poll.argtypes = [VP, ct.POINTER(ct.c_int64), ct.c_int64, ct.POINTER(ct.c_int64)]
         L.ufvm_service_set_admit_interval.argtypes = [VP, ct.c_int32]
         L.ufvm_service_set_schedule.argtypes = [VP, ct.c_int32, ct.c_int32]
+        L.ufvm_service_set_memory_budget.argtypes = [VP, ct.c_int64]
+        L.ufvm_service_admit.argtypes = [VP, ct.POINTER(ct.c_int32)]
+        L.ufvm_service_inject_admit_oom.argtypes = [VP, ct.c_int64, ct.c_int32]
         L._svc_ready = True
     return L
 
@@ -478,13 +481,30 @@ class Service:
     PHASES = ("update", "assemble_u", "solve_u", "correct_u", "assemble_p", "hierarchy", "solve_p", "correct_p")
 
     def stats(self) -> Dict:
-        out = np.zeros(17)
-        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 17))
+        out = np.zeros(25)
+        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 25))
         d = {f"{k}_ms": float(out[i]) for i, k in enumerate(self.PHASES)}
         d.update(u_sweeps=int(out[8]), p_cycles=int(out[9]), steps=int(out[10]), clock_ms=float(out[11]),
                  graph_ticks=int(out[12]), captures=int(out[13]), graph_launches=int(out[14]),
-                 cta_rows=int(out[15]), tunes=int(out[16]))
+                 cta_rows=int(out[15]), tunes=int(out[16]), resident_bytes=int(out[17]),
+                 memory_budget=int(out[18]), deferred_for_memory=int(out[19]), oom_requeues=int(out[20]),
+                 slot_drops=int(out[21]), footprint_scale=float(out[22]), u_loop_bodies=int(out[23]),
+                 p_loop_bodies=int(out[24]))
         return d
+
+    def admit(self) -> int:
+        """Admit queued cases now (uploads and processes their meshes); returns the active cases."""
+        n = ct.c_int32()
+        _check(_service_lib().ufvm_service_admit(self.h, ct.byref(n)))
+        return n.value
+
+    def inject_admit_oom(self, ticket: int, count: int = 1):
+        """Test hook: the next `count` admissions of `ticket` fail as an out-of-memory."""
+        _check(_service_lib().ufvm_service_inject_admit_oom(self.h, int(ticket), int(count)))
+
+    def set_memory_budget(self, nbytes: int):
+        """HBM budget (bytes) that admission keeps the resident cases and unreleased results in."""
+        _check(_service_lib().ufvm_service_set_memory_budget(self.h, int(nbytes)))
 
     def poll(self, capacity: int = 4096) -> List[int]:
         """Tickets finished since the previous poll."""

@@ -1,7 +1,8 @@
 """Generates the golden fixtures in this directory from the reference's own data files.
 
-Run in a container where the reference checkout exists (default path below, override with
-UFVM_REFERENCE). It reads only data the reference ships:
+Run where a checkout of the reference exists, with UFVM_REFERENCE set to its ``uFVM`` directory
+(the one holding ``src/`` and ``tutorials/``); the script refuses to run without it. It reads
+only data the reference ships:
 
 * ``tutorials/basic/cavity1/constant/polyMesh/theMesh.mat`` -- the fully processed mesh
   struct written by uFVM itself (utilities/extras/cfdGenerateInitialResults.m:16-23):
@@ -28,7 +29,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from matlab_ufvm_b200 import polymesh  # noqa: E402
 
-REF = os.environ.get("UFVM_REFERENCE", "/root/reference/uFVM")
+REF = os.environ.get("UFVM_REFERENCE", "")
 
 
 def the_mesh():
@@ -110,6 +111,8 @@ def cylinder():
 
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(os.path.join(REF, "tutorials")):
+        sys.exit("set UFVM_REFERENCE to the reference's uFVM directory (the one holding src/ and tutorials/)")
     the_mesh()
     polymesh_hashes()
     cylinder()

@@ -1,0 +1,116 @@
+"""The batched service against the FP64 oracle at the batch workload's own operating point.
+
+The cases are the pinned subset of the 512-case 2D cavity sweep (batched_sweep_params(512,
+seed=2024), QUIRKS_CONVERGING): for each grid point n in {16, 32, 64, 128, 256} x Re in
+{50, 500, 1000}, the sweep case nearest to it. The oracle side is tests/golden/sweep_oracle.json
+and sweep_oracle_fields.npz (written by make_sweep_oracle.py): the C++ oracle's own run of each
+case with the reference's solvers (V-cycle AMG with symmetric Gauss-Seidel for p, DILU for U),
+iterated to its fixed point, with the distance from that fixed point of the oracle's fields when
+the reference's residualControl test (booleans/cfdCheckConvergence.m:3-20, residuals as
+compute/cfdComputeNormalizedResidual.m:27-88) first passes at each tolerance.
+
+All pinned cases run together in one service (FP64 multicolour Gauss-Seidel for U, FP32
+agglomeration AMG preconditioning FP64 flexible CG for p), to the tight tolerance TIGHT, and the
+fields are also read at the tick where the residuals first pass 1e-6 -- the iterate at which the
+bench's runs stop. Field error is the relative L2 distance of U (all three components over the
+cells) and of p - p[cell 0] from the oracle's fixed point.
+
+Checked, per case:
+* at the 1e-6 stop, the service's field error is of the same size as the oracle's own at its
+  1e-6 stop (both are a few hundred times the residual; at most 4x the oracle's);
+* for n <= 128, the service's 1e-6 fields against the oracle's 1e-6 fields (the same stopping
+  rule on both sides) differ by less than the larger of the two stops' errors;
+* at TIGHT, the service's field error is <= 1e-6.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, rel
+from matlab_ufvm_b200 import case
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE = os.path.join(GOLDEN, "sweep_oracle.json")
+FIELDS = os.path.join(GOLDEN, "sweep_oracle_fields.npz")
+TIGHT = 1e-9          # residualControl of the tight run
+FIELD_TOL = 1e-6      # field error allowed at TIGHT
+SAME_SIZE = 4.0       # service error at the 1e-6 stop <= this x the oracle's own
+
+
+def _pinned():
+    with open(FIXTURE) as f:
+        d = json.load(f)
+    return [c for c in d["cases"] if c["pinned"] and "diverged_at" not in c and "6" in c["first"]]
+
+
+def run_pinned(ufvm, cases, fields, tol):
+    """All `cases` in one service to residualControl `tol`; returns per case the fields at the
+    first tick whose residuals are all <= 1e-6, the final fields and both iteration counts."""
+    specs = [case.cavity_case(c["n"], nu=1.0 / c["re"], quirks=case.QUIRKS_CONVERGING, tol_u=tol, tol_p=tol)
+             for c in cases]
+    svc = ufvm.Service(ufvm.fast_settings(specs[0]))
+    tickets = [svc.submit(s, 40000) for s in specs]
+    at6 = {}
+    done = set()
+    while len(done) < len(tickets):
+        svc.step()
+        for t, s in zip(tickets, specs):
+            if t in done:
+                continue
+            st = svc.status(t)
+            nc = s.mesh.n_cells
+            if t not in at6 and max(st["res"][:4]) <= 1e-6:
+                at6[t] = (svc.field(t, "U").reshape(3, -1)[:, :nc].copy(), svc.field(t, "p")[:nc].copy(),
+                          st["iterations"])
+            if st["state"] in ("converged", "stopped"):
+                done.add(t)
+    out = []
+    for c, t, s in zip(cases, tickets, specs):
+        st = svc.status(t)
+        assert st["state"] == "converged", (c["n"], c["re"], st)
+        nc = s.mesh.n_cells
+        out.append(dict(U6=at6[t][0], p6=at6[t][1], it6=at6[t][2], U=svc.field(t, "U").reshape(3, -1)[:, :nc],
+                        p=svc.field(t, "p")[:nc], it=st["iterations"]))
+    svc.close()
+    return out
+
+
+def _perr(p, pref):
+    return rel(p - p[0], pref - pref[0])
+
+
+def test_service_at_operating_point_against_oracle(ufvm_mod):
+    cases = _pinned()
+    assert len(cases) >= 12
+    z = np.load(FIELDS)
+    res = run_pinned(ufvm_mod, cases, z, TIGHT)
+    report = []
+    for c, r in zip(cases, res):
+        i = c["index"]
+        Uf = z[f"U_fix_{i}"].astype(np.float64)
+        pf = z[f"p_fix_{i}"].astype(np.float64)
+        row = {"index": i, "n": c["n"], "re": round(c["re"], 1),
+               "service_it_1e-6": r["it6"], "oracle_it_1e-6": c["first"]["6"],
+               "service_err_u_1e-6": rel(r["U6"], Uf), "service_err_p_1e-6": _perr(r["p6"], pf),
+               "oracle_err_u_1e-6": c["err_u"]["6"], "oracle_err_p_1e-6": c["err_p"]["6"],
+               "service_it_tight": r["it"], "service_err_u_tight": rel(r["U"], Uf),
+               "service_err_p_tight": _perr(r["p"], pf)}
+        if f"U_6_{i}" in z.files:
+            row["same_rule_u"] = rel(r["U6"], z[f"U_6_{i}"].astype(np.float64))
+            row["same_rule_p"] = _perr(r["p6"], z[f"p_6_{i}"].astype(np.float64))
+        report.append(row)
+    path = os.environ.get("UFVM_OPERATING_POINT_REPORT")
+    if path:
+        with open(path, "w") as f:
+            json.dump({"tight": TIGHT, "cases": report}, f, indent=1)
+    for row in report:
+        what = f"n={row['n']} Re={row['re']}"
+        assert row["service_err_u_tight"] <= FIELD_TOL and row["service_err_p_tight"] <= FIELD_TOL, (what, row)
+        assert row["service_err_u_1e-6"] <= SAME_SIZE * row["oracle_err_u_1e-6"] + FIELD_TOL, (what, row)
+        assert row["service_err_p_1e-6"] <= SAME_SIZE * row["oracle_err_p_1e-6"] + FIELD_TOL, (what, row)
+        if "same_rule_u" in row:
+            bound = max(row["service_err_u_1e-6"], row["oracle_err_u_1e-6"]) + FIELD_TOL
+            assert row["same_rule_u"] <= bound, (what, row)

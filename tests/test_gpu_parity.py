@@ -166,10 +166,13 @@ def test_stage_by_stage_bit_exact(ufvm_mod, oracle_mod, name):
 
 
 @pytest.mark.parametrize("name,iters", [("cavity20", 10), ("channel_small", 4), ("cylinder", 5),
-                                        ("cavity20_mcgs", 6)])
+                                        ("cavity20_mcgs", 6), ("cavity32_fcycle", 6), ("cavity32_fcycle_sor", 6)])
 def test_iterations_bit_exact(ufvm_mod, oracle_mod, name, iters):
     if name == "cavity20_mcgs":  # the multicolour smoother for U and p inside the AMG
         spec = case.CaseSpec(**{**case.cavity_case(20, nu=0.01).__dict__, "p_smoother": "MCGS", "u_smoother": "MCGS"})
+    elif name.startswith("cavity32_fcycle"):
+        # the F-cycle of solve/AMG/cfdApplyFCycle.m for p (ILU or Gauss-Seidel smoothing)
+        spec = case.cavity_case(32, nu=0.005, p_cycle="F-Cycle", p_smoother="SOR" if name.endswith("sor") else "ILU")
     else:
         spec = SPECS[name]()
     g = ufvm_mod.GpuCase(spec)

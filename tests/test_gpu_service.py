@@ -147,3 +147,90 @@ def test_service_channel_converges_to_oracle_fields(ufvm_mod, oracle_mod):
     nc = spec.mesh.n_cells
     assert rel(U.reshape(3, -1)[:, :nc], oc.get("U").reshape(3, -1)[:, :nc]) < 1e-6
     assert rel(p[:nc], oc.get("p")[:nc]) < 1e-6
+
+
+# ---- per-case failure handling (the reference stops a diverging case: top/cfdRunCase.m:124-127)
+def _solo(ufvm, spec):
+    st, U, p, _ = _run_alone(ufvm, spec)
+    return st, U, p
+
+
+def test_service_nan_case_fails_alone(ufvm_mod):
+    """A NaN planted on the host in one case's lid velocity (through the public submit call)
+    makes that case stop with UFVM_E_NAN; the two cases beside it in the batch finish with the
+    same bits as when they run alone."""
+    import dataclasses
+    good = [case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING),
+            case.cavity_case(24, nu=0.004, quirks=case.QUIRKS_CONVERGING)]
+    bad = case.cavity_case(20, nu=0.01, quirks=case.QUIRKS_CONVERGING)
+    vu = bad.val_u.copy()
+    vu[np.flatnonzero(vu[:, 0])[3], 0] = np.nan
+    bad = dataclasses.replace(bad, val_u=vu)
+    solo = [_solo(ufvm_mod, s) for s in good]
+    svc = ufvm_mod.Service(ufvm_mod.fast_settings(good[0]))
+    tickets = [svc.submit(good[0], 3000), svc.submit(bad, 3000), svc.submit(good[1], 3000)]
+    svc.run()
+    st_bad = svc.status(tickets[1])
+    assert st_bad["state"] == "stopped" and st_bad["status"] == 4, st_bad  # UFVM_E_NAN
+    for t, (st, U, p) in zip((tickets[0], tickets[2]), solo):
+        s2 = svc.status(t)
+        assert s2["state"] == "converged" and s2["iterations"] == st["iterations"]
+        assert np.array_equal(svc.field(t, "U"), U) and np.array_equal(svc.field(t, "p"), p)
+    svc.close()
+
+
+def test_service_admission_waits_for_memory(ufvm_mod):
+    """With an HBM budget below a queued case's footprint, that case waits at the head of the
+    queue (not failed) while the resident case runs, is admitted when the service empties, and
+    every case still finishes with its solo bits."""
+    specs = [case.cavity_case(20, nu=0.01, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(128, nu=0.01, quirks=case.QUIRKS_CONVERGING),
+             case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING)]
+    solo = [_solo(ufvm_mod, s) for s in specs]
+    svc = ufvm_mod.Service(ufvm_mod.fast_settings(specs[0]))
+    svc.set_memory_budget(24 << 20)  # room for the small cavities, not for the 128 x 128 one
+    tickets = [svc.submit(s, 3000) for s in specs]
+    nr, nq, _ = svc.step()
+    assert nr == 1 and nq == 2
+    assert svc.status(tickets[1])["state"] == "queued"
+    svc.run()
+    assert svc.stats()["deferred_for_memory"] > 0
+    for t, (st, U, p) in zip(tickets, solo):
+        s2 = svc.status(t)
+        assert s2["state"] == "converged" and s2["iterations"] == st["iterations"]
+        assert np.array_equal(svc.field(t, "U"), U) and np.array_equal(svc.field(t, "p"), p)
+    svc.close()
+
+
+def test_service_admission_oom_requeues_and_keeps_serving(ufvm_mod):
+    """A failed device allocation at admission (injected on the host) puts the request back at
+    the head of the queue while another case is resident; it is admitted at a later step and
+    converges with its solo bits. On an empty service the same failure stops that request with
+    UFVM_E_OOM, and the service goes on serving the next one."""
+    a = case.cavity_case(24, nu=0.01, quirks=case.QUIRKS_CONVERGING)
+    b = case.cavity_case(16, nu=0.005, quirks=case.QUIRKS_CONVERGING)
+    solo_b = _solo(ufvm_mod, b)
+    svc = ufvm_mod.Service(ufvm_mod.fast_settings(a))
+    ta = svc.submit(a, 3000)
+    svc.step()                      # a is resident
+    tb = svc.submit(b, 3000)
+    svc.inject_admit_oom(tb, 1)
+    svc.admit()                     # b's admission fails: back to the queue
+    assert svc.status(tb)["state"] == "queued"
+    assert svc.stats()["oom_requeues"] == 1
+    svc.run()
+    sb = svc.status(tb)
+    assert svc.status(ta)["state"] == "converged"
+    assert sb["state"] == "converged" and sb["iterations"] == solo_b[0]["iterations"]
+    assert np.array_equal(svc.field(tb, "U"), solo_b[1]) and np.array_equal(svc.field(tb, "p"), solo_b[2])
+    svc.close()
+
+    svc = ufvm_mod.Service(ufvm_mod.fast_settings(a))
+    t1 = svc.submit(b, 3000)
+    svc.inject_admit_oom(t1, 1)
+    t2 = svc.submit(b, 3000)
+    svc.run()
+    s1, s2 = svc.status(t1), svc.status(t2)
+    assert s1["state"] == "stopped" and s1["status"] == 3, s1  # UFVM_E_OOM
+    assert s2["state"] == "converged" and s2["iterations"] == solo_b[0]["iterations"]
+    svc.close()

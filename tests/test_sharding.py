@@ -45,6 +45,14 @@ def test_shards_partition_the_stream():
         sharding.stream_index(2, 2, 0)
 
 
+def test_batch_seeds_are_distinct_per_rank():
+    for world in (1, 2, 4, 8):
+        seeds = [sharding.batch_seed(r, world, 2024) for r in range(world)]
+        assert seeds[0] == 2024 and len(set(seeds)) == world
+    with pytest.raises(ValueError):
+        sharding.batch_seed(4, 4, 2024)
+
+
 def test_two_gloo_ranks_combine_measurements():
     world, n_total = 2, 37
     ctx = mp.get_context("spawn")
