@@ -48,6 +48,8 @@ SWEEP = 512
 SEED0 = 2024
 WARM_SEED = 1999
 ORACLE_FIXTURE = os.path.join(ROOT, "tests", "golden", "sweep_oracle.json")
+PLAIN_FIXTURE = os.path.join(ROOT, "tests", "golden", "sweep_oracle_plain.json")
+PLAIN_SETTINGS = {"p_smoother": "MCGS"}  # the plain form: V-cycle + multicolour GS for p, DILU for U
 
 
 def parse():
@@ -445,10 +447,10 @@ def load_peaks():
 
 
 # ------------------------------------------------------------------ the CPU arm (the oracle)
-def oracle_fixture():
+def oracle_fixture(path=ORACLE_FIXTURE):
     """The oracle on a stratified 64-case sample of the batch, converged on the machine that wrote
     the fixture: its own iteration counts and seconds to each residual decade."""
-    with open(ORACLE_FIXTURE) as f:
+    with open(path) as f:
         d = json.load(f)
     d["sample_cases"] = [c for c in d["cases"] if c["sample"]]
     return d
@@ -610,17 +612,19 @@ def _plain_first3(spec):
     return el
 
 
-def plain_batch_estimate(fix, here_t3: list) -> dict:
-    """The plain FP64 form (the reference's solvers, bit-exact with the oracle, so with the oracle's
-    iteration counts) one case at a time: each sample case's first three iterations are timed on
+def plain_batch_estimate(fix) -> dict:
+    """The plain FP64 form one case at a time: the reference's algorithm in FP64 on the GPU (AMG
+    rebuilt every p solve, V-cycle with multicolour Gauss-Seidel for p, level-scheduled DILU for U),
+    bit-exact with the oracle run with the same settings, so with that run's iteration counts
+    (tests/golden/sweep_oracle_plain.json). Each sample case's first three iterations are timed on
     the GPU and scaled by the fixture's measured time to convergence over its first three
     iterations' time; the batch's total is 512/64 of the sample's."""
     from matlab_ufvm_b200 import case
     sample = fix["sample_cases"]
-    _plain_first3(case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING))  # warm the path
+    _plain_first3(case.cavity_case(16, nu=0.01, quirks=case.QUIRKS_CONVERGING, **PLAIN_SETTINGS))  # warm the path
     times, conv, per_iter = [], 0, {}
     for c in sample:
-        spec = dataclasses.replace(base_spec(c["n"]), nu=1.0 / c["re"], tol_u=0.0, tol_p=0.0)
+        spec = dataclasses.replace(base_spec(c["n"]), nu=1.0 / c["re"], tol_u=0.0, tol_p=0.0, **PLAIN_SETTINGS)
         t3 = _plain_first3(spec)
         per_iter[str(c["n"])] = round(t3 / 3, 6)
         ratio = t3 / c["seconds_first3"]
@@ -630,8 +634,32 @@ def plain_batch_estimate(fix, here_t3: list) -> dict:
             times.append(c["seconds_to"]["6"] * ratio)
             conv += 1
     total = sum(times) * SWEEP / len(sample)
+    # model check: the smallest sample cases converged on the GPU, measured against the prediction
+    check = []
+    budget = 20.0
+    for c, pred in sorted(zip(sample, times), key=lambda x: x[1]):
+        if pred > budget or "diverged_at" in c or "6" not in c.get("first", {}):
+            continue
+        import torch
+        from matlab_ufvm_b200 import ufvm
+        spec = dataclasses.replace(base_spec(c["n"]), nu=1.0 / c["re"], **PLAIN_SETTINGS)
+        g = ufvm.GpuCase(spec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, _ = g.cfdRunCase(MAX_ITER)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        g.close()
+        check.append({"n": c["n"], "re": round(c["re"], 1), "iterations": it, "oracle_iterations": c["first"]["6"],
+                      "measured_s": round(el, 4), "predicted_s": round(pred, 4)})
+        budget -= el
+    ratios = [r["measured_s"] / r["predicted_s"] for r in check if r["predicted_s"] > 0]
     return {"cases_per_s": SWEEP * conv / len(sample) / total, "batch_seconds": total,
-            "s_per_iter_first3": per_iter}
+            "s_per_iter_first3": per_iter,
+            "model_check": {"cases": len(check),
+                            "iterations_match_oracle": all(r["iterations"] == r["oracle_iterations"] for r in check),
+                            "measured_over_predicted_median": statistics.median(ratios) if ratios else None,
+                            "rows": check}}
 
 
 def plain_kernel_rooflines(peaks, spec=None):
@@ -753,7 +781,7 @@ def main_ours(args):
             cpu["workers"] = workers
         if not args.no_plain:
             from matlab_ufvm_b200 import case
-            plain = plain_batch_estimate(fix, None) if fix else {}
+            plain = plain_batch_estimate(oracle_fixture(PLAIN_FIXTURE)) if os.path.exists(PLAIN_FIXTURE) else {}
             channel = case.channel_case()
             plain["kernels"] = plain_kernel_rooflines(peaks, channel)
             plain["named"] = plain_named_configs(channel)
@@ -781,12 +809,13 @@ def main_ours(args):
         if plain:
             line["plain_fp64_gpu"] = {
                 "value": plain.get("cases_per_s"), "unit": "cases/s",
-                "method": "plain FP64 form (the reference's V-cycle + Gauss-Seidel for p and DILU for U, AMG rebuilt "
-                          "every p solve, bit-exact with the oracle) one case at a time: each sample case's first "
-                          "3 iterations timed on the GPU, scaled by the oracle fixture's measured time to "
-                          "convergence over its first 3 iterations",
+                "method": "plain FP64 form one case at a time (the reference's AMG rebuilt every p solve, V-cycle "
+                          "with multicolour Gauss-Seidel for p, level-scheduled DILU for U; bit-exact with the oracle "
+                          "run with those settings): each of the 64 sample cases' first 3 iterations timed on the "
+                          "GPU, scaled by that oracle run's measured time to convergence over its first 3 "
+                          "iterations (tests/golden/sweep_oracle_plain.json)",
                 "batch_seconds": plain.get("batch_seconds"),
-                "s_per_iter_first3": plain.get("s_per_iter_first3"),
+                "s_per_iter_first3": plain.get("s_per_iter_first3"), "model_check": plain.get("model_check"),
                 "kernels_1M_tet_channel": plain["kernels"], "named_configs": plain["named"]}
             if plain.get("cases_per_s"):
                 line["batched_over_plain"] = value / plain["cases_per_s"]

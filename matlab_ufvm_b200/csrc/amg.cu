@@ -277,11 +277,15 @@ int agglomerate_level(LinCtx& c, AggScratch& w, Level& F, Level& C, int* nCoarse
   UFVM_CUDA(cudaMemsetAsync(w.newflag.p, 0, (n + 1) * sizeof(int), st));
   UFVM_CUDA(cudaMemsetAsync(w.resv.p, 0, n * sizeof(unsigned long long), st));
   AggArgs a{n, F.rowptr.p, F.col.p, w.strong.p, F.parents.p, w.status.p, w.resv.p, w.win.p, w.seedflag.p, c.iflag.p};
-  // Every round commits at least the lowest unprocessed seed, so n + 1 rounds bound it.
+  // Every round commits at least the lowest unprocessed seed, so n + 1 rounds bound it. The
+  // host reads the count of unprocessed seeds after batches of rounds that double in length
+  // (4, 8, 16, ... up to 64): a round after the last one finds no unprocessed seed and its
+  // kernels return at once, so a longer batch changes no result, only how often the host waits.
   unsigned int round = 0;
+  int batch = 4;
   for (;;) {
     int rem = 0;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < batch; ++k) {
       ++round;
       UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), st));
       k_agg_reserve<<<nblocks(n), kBlock, 0, st>>>(a, round);
@@ -293,16 +297,20 @@ int agglomerate_level(LinCtx& c, AggScratch& w, Level& F, Level& C, int* nCoarse
     UFVM_CUDA(cudaStreamSynchronize(st));
     if (rem == 0) break;
     if (round > (unsigned int)n + 8) { set_error("agglomeration rounds did not terminate"); return UFVM_E_INVALID; }
+    batch = std::min(2 * batch, 64);
   }
   // orphans
   k_is_orphan<<<nblocks(n), kBlock, 0, st>>>(n, F.parents.p, w.status.p /* isOrphan */, w.res0.p);
   UFVM_CUDA(cudaMemsetAsync(w.res1.p, 0, n * sizeof(int), st));
-  for (int r = 0;; ++r) {
-    UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), st));
-    k_orphan_round<<<nblocks(n), kBlock, 0, st>>>(n, F.rowptr.p, F.col.p, F.anb.p, w.maxAnb.p, w.status.p, w.res0.p,
-                                                  w.res1.p, F.parents.p, w.newflag.p, c.iflag.p);
+  // orphan rounds in batches as above (a round after the last finds every orphan resolved)
+  for (int r = 0, ob = 2;; ob = std::min(2 * ob, 32)) {
+    for (int k = 0; k < ob; ++k, ++r) {
+      UFVM_CUDA(cudaMemsetAsync(c.iflag.p, 0, sizeof(int), st));
+      k_orphan_round<<<nblocks(n), kBlock, 0, st>>>(n, F.rowptr.p, F.col.p, F.anb.p, w.maxAnb.p, w.status.p,
+                                                    w.res0.p, w.res1.p, F.parents.p, w.newflag.p, c.iflag.p);
+      UFVM_CUDA(cudaMemcpyAsync(w.res0.p, w.res1.p, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    }
     UFVM_LAUNCH_CHECK();
-    UFVM_CUDA(cudaMemcpyAsync(w.res0.p, w.res1.p, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
     int rem = 0;
     UFVM_CUDA(cudaMemcpyAsync(&rem, c.iflag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     UFVM_CUDA(cudaStreamSynchronize(st));
@@ -380,15 +388,54 @@ void AggScratch::release() {
 
 // ---------------------------------------------------------------------------------
 // AMG driver on a hierarchy whose level 0 is the assembled p matrix.
+// A rebuild (every p solve in the reference, cfdApplyAMG.m:19) keeps the previous hierarchy's
+// coarse-level device arrays and hands them to the new levels, whose allocations (dalloc) reuse an
+// array that is large enough instead of freeing and allocating it again; every schedule,
+// colouring and copy cached on a level is invalidated, since the new level's pattern may differ.
+static void reset_level_caches(Level& L) {
+  L.sched_valid = false;
+  L.nfwd = L.nbwd = L.maxw = 0;
+  L.dc_epoch = 0;
+  L.dc_quirks = 0;
+  for (int k = 0; k < 4; ++k) {
+    L.sell_valid[k] = false;
+    L.sellW[k] = 0;
+    L.sell_epoch[k] = 0;
+  }
+  L.color_valid = false;
+  L.ncolor = 0;
+  L.h_colorStart.clear();
+  L.mc_valid = false;
+  L.mcW = 0;
+  L.mc_epoch = 0;
+  L.ell_valid = false;
+  L.ellW = 0;
+}
+
 int AmgSolver::build(std::vector<Level>& lev, int max_coarse, int quirks, int* n_levels) {
-  for (size_t l = 1; l < lev.size(); ++l) free_level(lev[l]);
+  std::vector<Level> pool(lev.begin() + 1, lev.end());
   lev.resize(1);
+  size_t next = 0;
+  auto release_pool = [&]() {
+    for (size_t k = next; k < pool.size(); ++k) free_level(pool[k]);
+    pool.clear();
+  };
   int il = 0;
   while (il < max_coarse) {
     ++il;
     Level coarse;
+    if (next < pool.size()) {
+      coarse = pool[next];
+      pool[next++] = Level();
+      reset_level_caches(coarse);
+    }
     int np = 0;
-    UFVM_CHECK(agglomerate_level(ctx, agg, lev[il - 1], coarse, &np));
+    const int st = agglomerate_level(ctx, agg, lev[il - 1], coarse, &np);
+    if (st != UFVM_OK) {
+      free_level(coarse);
+      release_pool();
+      return st;
+    }
     if (np == 1 && !(quirks & UFVM_Q16_ONE_CELL_COARSEST)) {
       // repaired: a single aggregate of the pure-Neumann operator has a ~0 diagonal
       free_level(coarse);
@@ -398,6 +445,7 @@ int AmgSolver::build(std::vector<Level>& lev, int max_coarse, int quirks, int* n
     lev.push_back(coarse);
     if (np <= 5) break;
   }
+  release_pool();
   *n_levels = il + 1;
   return UFVM_OK;
 }

@@ -22,10 +22,15 @@ Two subsets of the sweep:
 A case on which the oracle diverges (a NaN residual: the reference's divergence test,
 top/cfdRunCase.m:124-127) is recorded with the iteration it diverged at and no fields.
 
+With --variant plain the same sample is run with the settings of the plain FP64 GPU form
+(multicolour Gauss-Seidel as the AMG smoother for p, the GPU path's UFVM_SMOOTHER_MCGS, whose
+restatement in the oracle is bit-exact with it; DILU for U as before), only to the tol = 1e-6
+stop, into sweep_oracle_plain.json: the iteration counts and times of the plain form's algorithm.
+
 Long-running (about two hours on 8 cores); per-case results are kept in --parts so an
 interrupted run resumes. Run from the repository root:
 
-    python tests/golden/make_sweep_oracle.py [--workers 7] [--parts DIR]
+    python tests/golden/make_sweep_oracle.py [--workers 7] [--parts DIR] [--variant plain]
 """
 from __future__ import annotations
 
@@ -73,13 +78,15 @@ def rel(a, b):
 
 
 def run_case(job):
-    idx, n, re, keep_fields, parts = job
+    idx, n, re, keep_fields, parts, variant = job
     path = os.path.join(parts, f"case{idx:03d}.npz")
     if os.path.exists(path):
         return idx
     from matlab_ufvm_b200 import case
     from oracle import oracle
-    spec = case.cavity_case(n, nu=1.0 / re, quirks=case.QUIRKS_CONVERGING, tol_u=0.0, tol_p=0.0)
+    extra = {"p_smoother": "MCGS"} if variant == "plain" else {}
+    decades = (6,) if variant == "plain" else DECADES
+    spec = case.cavity_case(n, nu=1.0 / re, quirks=case.QUIRKS_CONVERGING, tol_u=0.0, tol_p=0.0, **extra)
     oc = oracle.OracleCase(spec)
     nc = spec.mesh.n_cells
     snaps, first, t_first = {}, {}, {}
@@ -101,7 +108,7 @@ def run_case(job):
             os.replace(tmp, path)
             return idx
         worst = float(max(res[0], res[1], res[2], res[3]))
-        for k in DECADES:
+        for k in decades:
             if k not in first and worst <= 10.0 ** -k:
                 first[k] = it
                 t_first[k] = time.perf_counter() - t0
@@ -109,7 +116,7 @@ def run_case(job):
         if worst < 0.9 * best:
             best, best_it = worst, it
         i6 = first.get(6)
-        if len(first) == len(DECADES):
+        if len(first) == len(decades):
             break
         if i6 is not None and (it - best_it > 400 or it > 4 * i6 + 2000):
             break  # stagnated at the floating-point floor
@@ -142,12 +149,15 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workers", type=int, default=max(1, (os.cpu_count() or 2) - 1))
     ap.add_argument("--parts", default=os.path.join(tempfile.gettempdir(), "ufvm_sweep_oracle_parts"))
+    ap.add_argument("--variant", choices=("reference", "plain"), default="reference")
     args = ap.parse_args()
     os.makedirs(args.parts, exist_ok=True)
     params = sweep()
     sample, pinned = sample_indices(params), pinned_indices(params)
+    if args.variant == "plain":
+        pinned = []
     todo = sorted(set(sample) | set(pinned), key=lambda i: -(params[i][0] ** 3))
-    jobs = [(i, params[i][0], params[i][1], i in pinned, args.parts) for i in todo]
+    jobs = [(i, params[i][0], params[i][1], i in pinned, args.parts, args.variant) for i in todo]
     import multiprocessing as mp
     with mp.get_context("spawn").Pool(args.workers) as pool:
         for k, idx in enumerate(pool.imap_unordered(run_case, jobs)):
@@ -171,6 +181,14 @@ def main():
                           "diverged_at: the iteration whose residual was NaN. Written by make_sweep_oracle.py.",
            "sample": sample, "pinned": pinned, "grid_n": list(GRID_N), "grid_re": list(GRID_RE),
            "cases": cases}
+    if args.variant == "plain":
+        out["description"] = ("The oracle with the plain FP64 GPU form's settings (multicolour Gauss-Seidel as the "
+                              "AMG smoother for p, DILU for U) on the 64-case sample of the 512-case 2D cavity sweep, "
+                              "to the tol = 1e-6 stop; fields as in sweep_oracle.json. Written by "
+                              "make_sweep_oracle.py --variant plain.")
+        with open(os.path.join(HERE, "sweep_oracle_plain.json"), "w") as f:
+            json.dump(out, f, indent=0)
+        return
     with open(os.path.join(HERE, "sweep_oracle.json"), "w") as f:
         json.dump(out, f, indent=0)
     np.savez_compressed(os.path.join(HERE, "sweep_oracle_fields.npz"), **fields)
