@@ -73,6 +73,8 @@ def parse():
                          "mix of 2D/3D cavities and tet channels (its own JSON line)")
     ap.add_argument("--serving-requests", type=int, default=48, help="requests per serving phase")
     ap.add_argument("--capacity-steps", type=int, default=400, help="service steps of the closed-loop phase")
+    ap.add_argument("--serving-max-iter", type=int, default=8000,
+                    help="SIMPLE iteration limit of a serving request (the case script's endTime)")
     ap.add_argument("--plain-kernels", action="store_true",
                     help="only the plain FP64 form's solver-kernel rooflines on the 1M-cell tet channel (one JSON "
                          "line per kernel; the ncu target for those kernels)")
@@ -280,11 +282,17 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
             h2d += mesh_bytes(s)
     finished = {}
     remaining = len(specs)
+    tick_log = []  # (active cases before the tick, device ms of the tick)
+    clock = s0["clock_ms"]
+    active = len(specs)
     for _ in range(args.steps):
         for _ in range(args.ticks):
             if remaining == 0:
                 break
             nr, nq, _ = svc.step()
+            c1 = svc.stats()["clock_ms"]
+            tick_log.append((active, c1 - clock))
+            clock, active = c1, nr
             d2h += nr * STEP_D2H
             for t in svc.poll():
                 st = svc.status(t)
@@ -310,8 +318,22 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                graph_ticks=s1["graph_ticks"] - s0["graph_ticks"], ticks=s1["steps"] - s0["steps"],
                captures=s1["captures"] - s0["captures"], slot_drops=s1["slot_drops"] - s0["slot_drops"],
                peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
-               tickets=tickets)
+               tickets=tickets, tail=tail_profile(tick_log, len(specs)))
     return svc, out
+
+
+def tail_profile(tick_log, cases):
+    """How the batch's device time divides between ticks by the number of cases still active:
+    the tail of a fixed batch (its last, largest cases alone) is work at low occupancy."""
+    tot = sum(ms for _, ms in tick_log) or 1.0
+    bands = ((cases // 2, cases + 1), (cases // 8, cases // 2), (16, cases // 8), (0, 16))
+    out = []
+    for lo, hi in bands:
+        sel = [ms for a, ms in tick_log if lo <= a < hi]
+        out.append({"active_cases": f"{lo}-{hi - 1}", "ticks": len(sel), "ms": round(sum(sel), 1),
+                    "share": round(sum(sel) / tot, 4),
+                    "ms_per_tick_median": round(statistics.median(sel), 3) if sel else None})
+    return out
 
 
 ROOF_KERNEL = (1, "k_mc32_l0 (FP32 multicolour Gauss-Seidel sweep of the V-cycle's level 0, "
@@ -423,7 +445,7 @@ def roofline(svc, peaks, ticks: int = 12):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if not peaks.get("fallback")
             else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)",
             "tick_ms": round(tick_ms, 3), "u_sweeps_per_tick": round(us, 2), "p_cycles_per_tick": round(pc, 2),
-            "resident_cases": s1.get("resident_cases"), "kernels": rows}
+            "kernels": rows}
 
 
 def load_peaks():
@@ -800,6 +822,7 @@ def main_ours(args):
             "iterations": {"p50": pct(iters, 50), "max": max(iters) if iters else None},
             "ticks_timed": res["ticks"], "graph_ticks": res["graph_ticks"], "graph_captures": res["captures"],
             "slot_drops": res["slot_drops"], "resident_bytes_end": res["peak_bytes"],
+            "ticks_by_active_cases": res["tail"],
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res["clocks"],
         }
         if cpu:
@@ -863,7 +886,8 @@ def main_serving(args):
         return svc
 
     svc = service()
-    cap = serving.closed_loop_capacity(svc, cap_reqs, args.capacity_steps, spec_fn=spec_fn)
+    cap = serving.closed_loop_capacity(svc, cap_reqs, args.capacity_steps, spec_fn=spec_fn,
+                                       max_iter=args.serving_max_iter)
     cap["stats"] = {k: v for k, v in svc.stats().items() if k in ("resident_bytes", "memory_budget",
                                                                   "deferred_for_memory", "oom_requeues",
                                                                   "footprint_scale", "captures", "slot_drops")}
@@ -875,7 +899,7 @@ def main_serving(args):
     if rate > 0:
         svc = service()
         arr = serving.poisson_arrivals(len(open_reqs), rate, seed=303)
-        ol = serving.OpenLoop(svc, open_reqs, arr, spec_fn=spec_fn)
+        ol = serving.OpenLoop(svc, open_reqs, arr, spec_fn=spec_fn, max_iter=args.serving_max_iter)
         out = ol.run()
         line["open_loop_stats"] = {k: v for k, v in svc.stats().items() if k in (
             "resident_bytes", "memory_budget", "deferred_for_memory", "oom_requeues", "footprint_scale",

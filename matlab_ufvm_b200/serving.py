@@ -95,7 +95,11 @@ class Outcome:
     arrival_s: float
     late_s: float        # submission - arrival (at most one service step)
     queue_s: float
-    service_s: float     # admission to convergence
+    service_s: float     # admission to convergence (or to the stop)
+    size: tuple = ()
+    re: float = 0.0
+    status: int = 0      # ufvm_status of a stopped request
+    residuals: tuple = ()  # rms U1 U2 U3 p at the end
 
     @property
     def time_to_converge_s(self) -> float:
@@ -140,7 +144,9 @@ class OpenLoop:
             req, arr, sub = self.live.pop(t)
             st = self.svc.status(t)
             self.outcomes.append(Outcome(req.index, req.kind, st["state"], int(st["iterations"]), arr,
-                                         max(0.0, sub - arr), st["queue_ms"] * 1e-3, st["latency_ms"] * 1e-3))
+                                         max(0.0, sub - arr), st["queue_ms"] * 1e-3, st["latency_ms"] * 1e-3,
+                                         tuple(req.size), float(req.re), int(st.get("status", 0)),
+                                         tuple(float(x) for x in list(st.get("res", ()))[:4])))
             if self.release:
                 self.svc.release(t)
 
@@ -201,7 +207,10 @@ def summarize(outcomes: Sequence[Outcome]) -> Dict:
     conv = [o for o in outcomes if o.state == "converged"]
     span = (max(o.arrival_s + o.time_to_converge_s for o in conv) - min(o.arrival_s for o in outcomes)) \
         if conv else 0.0
-    return {"requests": len(outcomes), "converged": len(conv),
+    stopped = [{"index": o.index, "kind": o.kind, "size": list(o.size), "re": round(o.re, 1),
+                "iterations": o.iterations, "status": o.status, "rms_residuals": list(o.residuals)}
+               for o in outcomes if o.state != "converged"]
+    return {"requests": len(outcomes), "converged": len(conv), "stopped": stopped,
             "cases_per_s": len(conv) / span if span > 0 else 0.0,
             "time_to_converge_s": pcts([o.time_to_converge_s for o in conv]),
             "queue_s": pcts([o.late_s + o.queue_s for o in conv]),
