@@ -266,6 +266,11 @@ __device__ __forceinline__ void face_grad_corr(const MeshView& m, int fc, int o,
 //   k = 0, 1, 2: convection C1, C2, T;  3, 4, 5: diffusion C1, C2, T;  6: stress T.
 // The cell kernel below adds them exactly as the reference's scatter does.
 enum { UF_C1 = 0, UF_C2 = 1, UF_T = 2, UF_D1 = 3, UF_D2 = 4, UF_TD = 5, UF_TS = 6, UF_N = 7 };
+// Upwind convection coefficients of an interior face from its mass flux (sign +1): a function
+// of mdot alone, so the cell kernel recomputes them instead of reading them back (the same
+// operations give the same bits); uft[UF_C1] / uft[UF_C2] are written for boundary faces only.
+__device__ __forceinline__ double conv_c1(double psi) { return 1.0 * dmax(psi, 0.0); }
+__device__ __forceinline__ double conv_c2(double psi) { return -1.0 * dmax(-psi, 0.0); }
 
 __global__ void __launch_bounds__(kBlock, 3) k_uface(const SlotDesc* __restrict__ slots,
                                                      const int2* __restrict__ work, int comp) {
@@ -290,10 +295,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_uface(const SlotDesc* __restrict_
   if (fc < m.Fi) {
     const int o = m.owner[fc], n = m.neigh[fc];
     {  // (1) convection, sign +1
-      const double C1 = 1.0 * dmax(psi, 0.0);
-      const double C2 = -1.0 * dmax(-psi, 0.0);
+      const double C1 = conv_c1(psi);
+      const double C2 = conv_c2(psi);
       const double T = (C1 * ph[o] + C2 * ph[n]) + 0.0;
-      u[UF_C1 * F + fc] = C1; u[UF_C2 * F + fc] = C2; u[UF_T * F + fc] = T;
+      u[UF_T * F + fc] = T;  // C1, C2 of an interior face: recomputed from mdot by the cell kernel
     }
     const double w = m.gf[fc];
     const double gam = w * nu + (1 - w) * nu;
@@ -369,6 +374,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_uface(const SlotDesc* __restrict_
   u[UF_TS * F + fc] = (-1.0 * gam) * ((s0[b] * m.Sx[fc] + s1[b] * m.Sy[fc]) + s2[b] * m.Sz[fc]);
 }
 
+constexpr int kCellFaces = 8;  // cells with at most this many faces take the register path
+
 // cfdAssembleEquation('U', comp): the face terms of k_uface scattered into the cell's row in
 // the reference's order -- convection over the cell's faces, the convection divergence,
 // diffusion, explicit stress -- then grad(p), false transient, URF, scaled residual, DU.
@@ -387,53 +394,121 @@ __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restric
     const double* u = f.uft;
     const size_t F = (size_t)m.F;
     double acv = 0.0, bcv = 0.0, eff = 0.0;
-    // (1) convection, sign +1
-    for (int q = s; q < ne; ++q) {
-      const int fc = m.cfFace[q];
-      const double psi = f.mdot[fc];
-      const double C1 = u[UF_C1 * F + fc], T = u[UF_T * F + fc];
-      if (fc < m.Fi) {
-        const double C2 = u[UF_C2 * F + fc];
-        if (m.owner[fc] == e) { acv = acv + C1; anb[r0 + q - s] = 0.0 + C2; bcv = bcv - T; eff = eff + psi; }
-        else { acv = acv - C2; anb[r0 + q - s] = 0.0 - C1; bcv = bcv + T; eff = eff - psi; }
-      } else {
-        acv = acv + C1;
-        bcv = bcv - T;
-        eff = eff + psi;
+    const int nf = ne - s;
+    if (nf <= kCellFaces) {
+      // The cell's face list, its side of each face (owner, neighbour, boundary) and its row of
+      // off-diagonals are read or built once and kept in registers; the three passes below add
+      // the same terms in the same order as the general loops after them.
+      int fcs[kCellFaces], side[kCellFaces];
+      double an[kCellFaces];
+#pragma unroll
+      for (int j = 0; j < kCellFaces; ++j)
+        if (j < nf) {
+          fcs[j] = m.cfFace[s + j];
+          side[j] = fcs[j] < m.Fi ? (m.owner[fcs[j]] == e ? 1 : -1) : 0;
+        }
+      // (1) convection, sign +1
+#pragma unroll
+      for (int j = 0; j < kCellFaces; ++j)
+        if (j < nf) {
+          const int fc = fcs[j];
+          const double psi = f.mdot[fc];
+          const double T = u[UF_T * F + fc];
+          if (side[j] > 0) {
+            const double C2 = conv_c2(psi);
+            acv = acv + conv_c1(psi); an[j] = 0.0 + C2; bcv = bcv - T; eff = eff + psi;
+          } else if (side[j] < 0) {
+            const double C2 = conv_c2(psi);
+            acv = acv - C2; an[j] = 0.0 - conv_c1(psi); bcv = bcv + T; eff = eff - psi;
+          } else {
+            acv = acv + u[UF_C1 * F + fc]; bcv = bcv - T; eff = eff + psi;
+          }
+        }
+      {  // cfdAssembleConvectionDivergenceTerm
+        const double fce = dmax(eff, 0.0) - eff;
+        const double fve = -dmax(eff, 0.0) * ph[e];
+        const double fte = fce * ph[e] + fve;
+        acv = acv + fce;
+        bcv = bcv - fte;
       }
-    }
-    {  // cfdAssembleConvectionDivergenceTerm
-      const double fce = dmax(eff, 0.0) - eff;
-      const double fve = -dmax(eff, 0.0) * ph[e];
-      const double fte = fce * ph[e] + fve;
-      acv = acv + fce;
-      bcv = bcv - fte;
-    }
-    // (2) diffusion, sign -1
-    for (int q = s; q < ne; ++q) {
-      const int fc = m.cfFace[q];
-      const double C1 = u[UF_D1 * F + fc], T = u[UF_TD * F + fc];
-      if (fc < m.Fi) {
-        const double C2 = u[UF_D2 * F + fc];
-        const int k = r0 + q - s;
-        if (m.owner[fc] == e) { acv = acv + C1; anb[k] = anb[k] + C2; bcv = bcv - T; }
-        else { acv = acv - C2; anb[k] = anb[k] - C1; bcv = bcv + T; }
-      } else {
-        acv = acv + C1;
-        bcv = bcv - T;
+      // (2) diffusion, sign -1
+#pragma unroll
+      for (int j = 0; j < kCellFaces; ++j)
+        if (j < nf) {
+          const int fc = fcs[j];
+          const double C1 = u[UF_D1 * F + fc], T = u[UF_TD * F + fc];
+          if (side[j] > 0) {
+            const double C2 = u[UF_D2 * F + fc];
+            acv = acv + C1; an[j] = an[j] + C2; bcv = bcv - T;
+          } else if (side[j] < 0) {
+            const double C2 = u[UF_D2 * F + fc];
+            acv = acv - C2; an[j] = an[j] - C1; bcv = bcv + T;
+          } else {
+            acv = acv + C1; bcv = bcv - T;
+          }
+        }
+      // (3) explicit stress, sign -1
+#pragma unroll
+      for (int j = 0; j < kCellFaces; ++j)
+        if (j < nf) {
+          const double T = u[UF_TS * F + fcs[j]];
+          if (side[j] > 0) { acv = acv + 0.0; an[j] = an[j] + 0.0; bcv = bcv - T; }
+          else if (side[j] < 0) { acv = acv - 0.0; an[j] = an[j] - 0.0; bcv = bcv + T; }
+          else { acv = acv + 0.0; bcv = bcv - T; }
+        }
+#pragma unroll
+      for (int j = 0; j < kCellFaces; ++j)
+        if (j < nf && side[j] != 0) anb[r0 + j] = an[j];
+    } else {
+      // (1) convection, sign +1
+      for (int q = s; q < ne; ++q) {
+        const int fc = m.cfFace[q];
+        const double psi = f.mdot[fc];
+        const double T = u[UF_T * F + fc];
+        const double C1 = fc < m.Fi ? conv_c1(psi) : u[UF_C1 * F + fc];
+        if (fc < m.Fi) {
+          const double C2 = conv_c2(psi);
+          if (m.owner[fc] == e) { acv = acv + C1; anb[r0 + q - s] = 0.0 + C2; bcv = bcv - T; eff = eff + psi; }
+          else { acv = acv - C2; anb[r0 + q - s] = 0.0 - C1; bcv = bcv + T; eff = eff - psi; }
+        } else {
+          acv = acv + C1;
+          bcv = bcv - T;
+          eff = eff + psi;
+        }
       }
-    }
-    // (3) explicit stress, sign -1
-    for (int q = s; q < ne; ++q) {
-      const int fc = m.cfFace[q];
-      const double T = u[UF_TS * F + fc];
-      if (fc < m.Fi) {
-        const int k = r0 + q - s;
-        if (m.owner[fc] == e) { acv = acv + 0.0; anb[k] = anb[k] + 0.0; bcv = bcv - T; }
-        else { acv = acv - 0.0; anb[k] = anb[k] - 0.0; bcv = bcv + T; }
-      } else {
-        acv = acv + 0.0;
-        bcv = bcv - T;
+      {  // cfdAssembleConvectionDivergenceTerm
+        const double fce = dmax(eff, 0.0) - eff;
+        const double fve = -dmax(eff, 0.0) * ph[e];
+        const double fte = fce * ph[e] + fve;
+        acv = acv + fce;
+        bcv = bcv - fte;
+      }
+      // (2) diffusion, sign -1
+      for (int q = s; q < ne; ++q) {
+        const int fc = m.cfFace[q];
+        const double C1 = u[UF_D1 * F + fc], T = u[UF_TD * F + fc];
+        if (fc < m.Fi) {
+          const double C2 = u[UF_D2 * F + fc];
+          const int k = r0 + q - s;
+          if (m.owner[fc] == e) { acv = acv + C1; anb[k] = anb[k] + C2; bcv = bcv - T; }
+          else { acv = acv - C2; anb[k] = anb[k] - C1; bcv = bcv + T; }
+        } else {
+          acv = acv + C1;
+          bcv = bcv - T;
+        }
+      }
+      // (3) explicit stress, sign -1
+      for (int q = s; q < ne; ++q) {
+        const int fc = m.cfFace[q];
+        const double T = u[UF_TS * F + fc];
+        if (fc < m.Fi) {
+          const int k = r0 + q - s;
+          if (m.owner[fc] == e) { acv = acv + 0.0; anb[k] = anb[k] + 0.0; bcv = bcv - T; }
+          else { acv = acv - 0.0; anb[k] = anb[k] - 0.0; bcv = bcv + T; }
+        } else {
+          acv = acv + 0.0;
+          bcv = bcv - T;
+        }
       }
     }
     // (4) grad(p), sign +1 (cfdAssemblePressureGradientTerm.m:11-40)
