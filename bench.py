@@ -317,6 +317,7 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                launches=s1["graph_launches"] - s0["graph_launches"],
                graph_ticks=s1["graph_ticks"] - s0["graph_ticks"], ticks=s1["steps"] - s0["steps"],
                captures=s1["captures"] - s0["captures"], slot_drops=s1["slot_drops"] - s0["slot_drops"],
+               host_ms={k: round(s1[k] - s0[k], 1) for k in ("host_rebuild_ms", "host_capture_ms", "host_drop_ms")},
                peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
                tickets=tickets, tail=tail_profile(tick_log, len(specs)))
     return svc, out
@@ -822,7 +823,8 @@ def main_ours(args):
             "iterations": {"p50": pct(iters, 50), "max": max(iters) if iters else None},
             "ticks_timed": res["ticks"], "graph_ticks": res["graph_ticks"], "graph_captures": res["captures"],
             "slot_drops": res["slot_drops"], "resident_bytes_end": res["peak_bytes"],
-            "ticks_by_active_cases": res["tail"],
+            "ticks_by_active_cases": res["tail"], "host_ms_in_timed_region": res["host_ms"],
+            "device_ms_in_ticks": round(sum(b["ms"] for b in res["tail"]), 1),
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res["clocks"],
         }
         if cpu:

@@ -221,9 +221,10 @@ int ufvm_agglomerate_level(int32_t n, const int32_t* rowptr, const int32_t* col,
  * allocate at admission waits at the head of the queue while other cases are resident. Every
  * resident case advances one SIMPLE iteration per ufvm_service_step in one launch per stage,
  * and a case finishes when it converges (residualControl), fails, or reaches its iteration
- * limit; its result (U, p, mdot at that iteration) is kept on the device until release, and its
- * own memory is freed when its slot leaves the batch (gathered with the next admission, or when
- * finished slots reach 1/16 of the active cells or 32 steps), freeing room for queued cases. The solver settings are shared by all
+ * limit; its result (U, p, mdot at that iteration) is kept on the device until release. Its slot
+ * leaves the batch with the next admission, or when the device time spent on finished slots
+ * reaches the host cost of a rebuild, or after 256 steps; its own device memory is freed when an
+ * admission needs the room (or at ufvm_service_destroy). The solver settings are shared by all
  * cases of a service; nu, the boundary data and the pressure reference cell are per case (a
  * case whose boundaries are all walls, empty or symmetry planes pins p at settings->
  * fixed_element, or cell 0 if that is negative; any other case has none, cfdReadSystem.m:
@@ -250,8 +251,9 @@ int ufvm_service_release(ufvm_service* s, int64_t ticket);
  * V-cycle, the number of completed autotuning passes, the HBM bytes held by the slots and the
  * unreleased results, the memory budget, the admissions deferred for memory, the admissions
  * that failed to allocate and were re-queued, the departures of finished slots from the batch,
- * the footprint estimate's scale, and the U-smoother and p-cycle loop bodies the replayed ticks
- * have run. Writes min(n, 25) values. */
+ * the footprint estimate's scale, the U-smoother and p-cycle loop bodies the replayed ticks
+ * have run, and the host time (ms) spent rebuilding slot tables, capturing tick graphs and
+ * freeing departed cases. Writes min(n, 28) values. */
 int ufvm_service_stats(ufvm_service* s, double* out, int n);
 /* Admits queued cases now, as far as the budgets allow, without waiting for the next step: their
  * meshes are uploaded and processed on the service stream, so a caller can have a batch resident

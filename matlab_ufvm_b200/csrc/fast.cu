@@ -18,6 +18,7 @@
 // A step without hierarchy builds is captured once and replayed as a CUDA graph whose solve
 // loops are conditional WHILE nodes ended on the device.
 #include <algorithm>
+#include <chrono>
 
 #include "fast.cuh"
 
@@ -1523,7 +1524,15 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
     if (!c->lev[0].color_valid) { UFVM_CHECK(build_coloring(c->lin, c->lev[0])); tables_dirty = true; }
     c->dev_bytes += t_dev_bytes - b0;
   }
-  if (tables_dirty) UFVM_CHECK(rebuild_tables());
+  auto host_ms_since = [](std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+  };
+  double rebuild_ms = 0.0;
+  if (tables_dirty) {
+    const auto h0 = std::chrono::steady_clock::now();
+    UFVM_CHECK(rebuild_tables());
+    rebuild_ms = host_ms_since(h0);
+  }
   ++n_iter_calls;
   // a tick without hierarchy builds runs as one graph launch (captured when the tables change)
   bool g = use_graph != 0;
@@ -1543,14 +1552,22 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
         return UFVM_E_CUDA;
       }
     }
-    if (!graph_valid && capture_tick() != UFVM_OK) {
-      // keep serving: this and later ticks are launched eagerly
-      std::fprintf(stderr, "ufvm: capturing the tick graph failed (%s); ticks are launched eagerly\n", get_error());
-      cudaGetLastError();
-      use_graph = 0;
-      g = false;
+    if (!graph_valid) {
+      const auto h1 = std::chrono::steady_clock::now();
+      const int cst = capture_tick();
+      const double cms = host_ms_since(h1);
+      host_capture_ms += cms;
+      last_rebuild_ms = rebuild_ms + cms;  // the host cost of a change of the slot set
+      if (cst != UFVM_OK) {
+        // keep serving: this and later ticks are launched eagerly
+        std::fprintf(stderr, "ufvm: capturing the tick graph failed (%s); ticks are launched eagerly\n", get_error());
+        cudaGetLastError();
+        use_graph = 0;
+        g = false;
+      }
     }
   }
+  host_rebuild_ms += rebuild_ms;
   if (g) {
     UFVM_CUDA(cudaGraphLaunch(gexec, stream));
     for (auto* c : cases) c->p_solves += S.n_correctors;

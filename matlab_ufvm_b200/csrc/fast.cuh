@@ -125,6 +125,9 @@ struct Service {
   cudaStream_t bstream = nullptr;      // loop bodies are captured on this stream
   cudaStream_t main_stream = nullptr;
   long long n_graph_ticks = 0, n_captures = 0;
+  // host time (ms) spent rebuilding the slot tables and capturing the tick graph, in total and
+  // for the most recent change of the slot set
+  double host_rebuild_ms = 0.0, host_capture_ms = 0.0, last_rebuild_ms = 0.0;
   // kernel launches: kernels of the captured tick outside the loops and per loop body, and
   // the device counters of executed U / p loop bodies
   long long static_kernels = 0, ubody_kernels = 0, pbody_kernels = 0, launches_total = 0;

@@ -9,17 +9,25 @@
 //
 // A finished case keeps its slot in the batch, frozen, until the slots are next rebuilt: its
 // result (U, p, mdot at the finishing iteration) is copied to a snapshot on the device, and the
-// case may run a few more iterations that nobody reads. Rebuilding the slot tables re-captures the
+// case may run more iterations that nobody reads. Rebuilding the slot tables re-captures the
 // tick's CUDA graph, so departures are gathered: the frozen slots are dropped when queued cases
-// are admitted, when their cells pass 1/16 of the active cells, when one has waited 32 steps, or
-// when no active case is left.
+// are admitted, when the device time spent on them since they froze (their share of each tick, by
+// cells) reaches the host time the last drop and rebuild took, when one has waited
+// kMaxFrozenSteps steps, or when no active case is left. A departed case's device memory is
+// freed later, when admission finds too little free memory or the service ends: cudaFree waits
+// for the whole device, and freeing every case at its departure cost more host time than the
+// rest of the departures together.
 #include <deque>
 #include <map>
 #include <memory>
 
+#include <chrono>
+
 #include "fast.cuh"
 
 namespace ufvm {
+
+constexpr int kMaxFrozenSteps = 256;  // a finished case leaves the batch at the latest after this
 
 struct Pending {
   long long ticket;
@@ -64,6 +72,18 @@ struct ServiceImpl {
   std::vector<char> frozen;     // per slot of svc.cases: finished, result in its snapshot
   std::vector<int> frozen_age;  // steps since the slot froze
   bool force_drop = false;
+  // departures are gathered while the work spent on frozen slots (their share of each tick's
+  // device time) stays below what dropping them costs on the host (the last rebuild of the slot
+  // tables with its graph capture, plus freeing the departed cases)
+  double waste_ms = 0.0, last_drop_ms = 0.0, host_drop_ms = 0.0;
+  // Cases that left the batch are not freed at once: freeing a case's device arrays
+  // (cudaFree, which waits for the whole device) costs far more host time than the rest of a
+  // departure. They wait here until admission finds too little memory, or the service ends.
+  std::vector<Case*> graveyard;
+  void bury() {
+    for (Case* c : graveyard) delete c;
+    graveyard.clear();
+  }
   std::map<long long, int> inject_oom;  // fault injection: admissions of a ticket that fail as OOM
   double clock_ms = 0;  // accumulated device time of all steps
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -84,6 +104,7 @@ struct ServiceImpl {
   std::vector<int> tune_n;
   std::vector<long long> finished_unpolled;  // tickets finished since the last poll
   ~ServiceImpl() {
+    bury();
     for (auto& kv : rec) {
       // ufvm_service_destroy has cleared the cases that hold slots (the Service frees those)
       if (kv.second.c) delete kv.second.c;
@@ -132,9 +153,19 @@ static void fill_desc(const Pending& p, ufvm_mesh_desc& d) {
   d.patch_n = p.pn.data();
 }
 
+static void drop_frozen_(ServiceImpl& S);
+
 // Finished slots leave the batch: each case's memory is freed (its result lives in its
 // snapshot) and the slot tables are rebuilt at the next iteration.
 static void drop_frozen(ServiceImpl& S) {
+  const auto t0 = std::chrono::steady_clock::now();
+  drop_frozen_(S);
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  S.host_drop_ms += ms;
+  S.last_drop_ms = ms;
+}
+
+static void drop_frozen_(ServiceImpl& S) {
   Service& V = S.svc;
   std::vector<Case*> keep;
   std::vector<long long> keept;
@@ -149,11 +180,11 @@ static void drop_frozen(ServiceImpl& S) {
     any = true;
     auto it = S.rec.find(V.tickets[q]);
     Record& r = it->second;
-    if (r.released) {  // nobody will read it: free the case and forget the ticket
-      delete V.cases[q];
+    if (r.released) {  // nobody will read it: the case goes to be freed, the ticket is forgotten
+      S.graveyard.push_back(V.cases[q]);
       S.rec.erase(it);
-    } else if (r.snap.U) {  // the snapshot holds the result: free the case
-      delete V.cases[q];
+    } else if (r.snap.U) {  // the snapshot holds the result: the case goes to be freed
+      S.graveyard.push_back(V.cases[q]);
       r.c = nullptr;
     }  // else the record keeps the case (its fields are the result)
   }
@@ -162,6 +193,7 @@ static void drop_frozen(ServiceImpl& S) {
   V.tables_dirty = true;
   ++S.n_drops;
   S.force_drop = false;
+  S.waste_ms = 0.0;
 }
 
 static bool admission_due(const ServiceImpl& S) {
@@ -180,7 +212,14 @@ static int admit(ServiceImpl& S) {
       if (S.resident_cells + p.cells > S.max_cells) break;
       if (S.slot_bytes() + S.snap_bytes + est > S.max_bytes) { ++S.n_deferred_mem; break; }
       size_t fr = 0, tot = 0;
-      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (long long)fr < est + (est >> 3)) { ++S.n_deferred_mem; break; }
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (long long)fr < est + (est >> 3)) {
+        if (!S.graveyard.empty()) {  // free the departed cases, then look again
+          S.bury();
+          continue;
+        }
+        ++S.n_deferred_mem;
+        break;
+      }
     }
     ufvm_mesh_desc d;
     fill_desc(p, d);
@@ -196,17 +235,25 @@ static int admit(ServiceImpl& S) {
     Case* c = new Case();
     const long long b0 = t_dev_bytes;
     int st;
+    bool injected = false;
     auto inj = S.inject_oom.find(p.ticket);
     if (inj != S.inject_oom.end() && inj->second > 0) {  // a failed device allocation, injected
       --inj->second;
       set_error("cudaMalloc: out of memory (injected)");
       st = UFVM_E_OOM;
+      injected = true;
     } else {
       st = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr, nullptr,
                             nullptr, S.svc.stream);
     }
     c->dev_bytes = t_dev_bytes - b0;
     Record& r = S.rec[p.ticket];
+    if (st == UFVM_E_OOM && !injected && !S.graveyard.empty()) {  // room held by departed cases: free it, retry
+      delete c;
+      cudaGetLastError();
+      S.bury();
+      continue;
+    }
     if (st == UFVM_E_OOM && !S.svc.cases.empty()) {
       // the device is full after all: the request waits at the head of the queue for memory
       delete c;
@@ -400,18 +447,18 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
   ServiceImpl& S = h->impl;
   Service& V = S.svc;
   {
-    // gather departures: drop the frozen slots when they hold a sixteenth of the active cells,
-    // when one has waited 32 steps, when no active case is left, or after a failure
-    long long fcells = 0;
+    // gather departures: drop the frozen slots once the device time they have taken since they
+    // froze reaches the host cost of dropping them, when one has waited kMaxFrozenSteps steps,
+    // when no active case is left, or after a failure (admission drops them too)
     int oldest = 0;
     bool anyf = false;
     for (size_t q = 0; q < V.cases.size(); ++q)
       if (S.frozen[q]) {
         anyf = true;
-        fcells += S.rec[V.tickets[q]].cells;
         oldest = std::max(oldest, S.frozen_age[q]);
       }
-    if (anyf && (S.force_drop || 16 * fcells >= S.resident_cells || oldest >= 32 || S.resident_cells == 0))
+    if (anyf && (S.force_drop || S.waste_ms >= V.last_rebuild_ms + S.last_drop_ms || oldest >= kMaxFrozenSteps ||
+                 S.resident_cells == 0))
       drop_frozen(S);
   }
   UFVM_CHECK(admit(S));
@@ -429,6 +476,12 @@ int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, i
     UFVM_CUDA(cudaEventElapsedTime(&ms, S.e0, S.e1));
     S.clock_ms += ms;
     tune_step(S, ms, V.n_graph_ticks != graph_before);
+    {  // the share of this tick spent on frozen slots (work in proportion to cells)
+      long long fcells = 0;
+      for (size_t q = 0; q < V.cases.size(); ++q)
+        if (S.frozen[q]) fcells += S.rec[V.tickets[q]].cells;
+      if (fcells > 0) S.waste_ms += ms * (double)fcells / (double)(fcells + S.resident_cells);
+    }
     for (size_t q = 0; q < V.cases.size(); ++q) {
       if (S.frozen[q]) { ++S.frozen_age[q]; continue; }
       Record& r = S.rec[V.tickets[q]];
@@ -565,6 +618,9 @@ int ufvm_service_stats(ufvm_service* h, double* out, int n) {
   v.push_back(h->impl.est_scale);
   v.push_back((double)V.loops_seen[0]);  // U smoother loop bodies run by replayed ticks
   v.push_back((double)V.loops_seen[1]);  // p V-cycle loop bodies run by replayed ticks
+  v.push_back(V.host_rebuild_ms);
+  v.push_back(V.host_capture_ms);
+  v.push_back(h->impl.host_drop_ms);
   for (int i = 0; i < n; ++i) out[i] = i < (int)v.size() ? v[i] : 0.0;
   return UFVM_OK;
 }
