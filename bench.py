@@ -264,9 +264,14 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
     stream = torch.cuda.ExternalStream(svc.stream())
     h2d = d2h = 0
     tickets = []
+    admit_s = None
     if not e2e:
         tickets = [svc.submit(s, MAX_ITER) for s in specs]
+        torch.cuda.synchronize()
+        a0 = time.perf_counter()
         svc.admit()
+        torch.cuda.synchronize()
+        admit_s = time.perf_counter() - a0
     torch.cuda.synchronize()
     barrier(ws)
     clk = ClockSampler(torch.cuda.current_device()) if rank == 0 and not e2e else None
@@ -319,7 +324,8 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                captures=s1["captures"] - s0["captures"], slot_drops=s1["slot_drops"] - s0["slot_drops"],
                host_ms={k: round(s1[k] - s0[k], 1) for k in ("host_rebuild_ms", "host_capture_ms", "host_drop_ms")},
                peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
-               tickets=tickets, tail=tail_profile(tick_log, len(specs)))
+               tickets=tickets, tail=tail_profile(tick_log, len(specs)), admit_s=admit_s,
+               first_tick_ms=tick_log[0][1] if tick_log else None)
     return svc, out
 
 
@@ -825,6 +831,8 @@ def main_ours(args):
             "slot_drops": res["slot_drops"], "resident_bytes_end": res["peak_bytes"],
             "ticks_by_active_cases": res["tail"], "host_ms_in_timed_region": res["host_ms"],
             "device_ms_in_ticks": round(sum(b["ms"] for b in res["tail"]), 1),
+            "admission_s_before_timing": round(res["admit_s"], 3) if res["admit_s"] is not None else None,
+            "first_tick_ms": res["first_tick_ms"],
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res["clocks"],
         }
         if cpu:

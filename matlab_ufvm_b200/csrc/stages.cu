@@ -272,7 +272,7 @@ enum { UF_C1 = 0, UF_C2 = 1, UF_T = 2, UF_D1 = 3, UF_D2 = 4, UF_TD = 5, UF_TS = 
 __device__ __forceinline__ double conv_c1(double psi) { return 1.0 * dmax(psi, 0.0); }
 __device__ __forceinline__ double conv_c2(double psi) { return -1.0 * dmax(-psi, 0.0); }
 
-__global__ void __launch_bounds__(kBlock, 3) k_uface(const SlotDesc* __restrict__ slots,
+__global__ void __launch_bounds__(kBlock, 4) k_uface(const SlotDesc* __restrict__ slots,
                                                      const int2* __restrict__ work, int comp) {
   SLOT_BEGIN(work);
   const int fc = idx;
