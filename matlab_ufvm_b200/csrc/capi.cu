@@ -514,7 +514,12 @@ int ufvm_profile_plain_kernel(int32_t kernel, int32_t n, const int32_t* rowptr, 
     if (kernel == 1 || kernel == 3) UFVM_CHECK(check_barrier(c));
     *ms_per_launch = total / reps;
     const double pass = 36.0 * n + 12.0 * nnz;  // one read of the system and x, one vector written
-    *bytes_per_launch = kernel == 0 ? pass : kernel == 3 ? pass + 40.0 * n + 24.0 * nnz : 2.0 * pass;
+    double sweep = 2.0 * pass;
+    if (kernel == 2 && L.ncolor > 0) {  // the backward pass skips the repeated last colour's rows
+      const double last = (double)(L.h_colorStart[L.ncolor] - L.h_colorStart[L.ncolor - 1]);
+      sweep -= 36.0 * last + 12.0 * nnz * (last / n);
+    }
+    *bytes_per_launch = kernel == 0 ? pass : kernel == 3 ? pass + 40.0 * n + 24.0 * nnz : sweep;
     return UFVM_OK;
   };
   const int st = body();

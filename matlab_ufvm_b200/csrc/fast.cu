@@ -501,6 +501,26 @@ __device__ __forceinline__ void restrict_row32(const LevDesc& F, const LevDesc& 
   C.x[P] = 0.0f;
 }
 
+// The same restriction with each child's residual formed in place (the same operations as
+// res_row32, so the same values) instead of read back from F.r: used where nothing else reads
+// F.r, it saves a pass over the level and the barrier between the two.
+__device__ __forceinline__ void restrict_res_row32(const LevDesc& F, const LevDesc& C, int P) {
+  float v = 0.0f;
+  if (F.pmode) {
+    for (int q = F.childStartP[P]; q < F.childStartP[P + 1]; ++q) {
+      const int p = F.childP[q];
+      v = v + row_sum32(F, p, F.bc[p] - F.ac[p] * F.x[p]);
+    }
+  } else {
+    for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) {
+      const int p = F.child[q];
+      v = v + row_sum32(F, p, F.bc[p] - F.ac[p] * F.x[p]);
+    }
+  }
+  C.bc[P] = v;
+  C.x[P] = 0.0f;
+}
+
 __device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C, int p) {
   F.x[p] = F.x[p] + F.pw * C.x[F.pmode ? F.parentsP[p] : F.parents[p]];
 }
@@ -704,11 +724,15 @@ __device__ void coarse_apply(const LevDesc& A, const double* __restrict__ X, con
   d.sync();
 }
 
+// A symmetric multicolour sweep runs the colours forward and then backward. The backward pass
+// starts at colour C-1, which the forward pass has just updated from the same neighbour values
+// (rows of one colour are not coupled, and a row's update x = (b - sum anb x_nb) / a does not
+// read its own x), so that update would write the same bits again: every sweep below skips it.
 template <class D>
 __device__ void smooth_dom(const LevDesc& A, int sweeps, const D& d) {
   for (int sw = 0; sw < sweeps; ++sw)
     for (int pass = 0; pass < 2; ++pass)
-      for (int q = 0; q < A.ncolor; ++q) {
+      for (int q = pass; q < A.ncolor; ++q) {
         const int c = pass == 0 ? q : A.ncolor - 1 - q;
         const int cnt = A.colorStart[c + 1] - A.colorStart[c];
         for (int t = d.tid; t < cnt; t += d.nth) gs_row32(A, color_row(A, c, t));
@@ -726,9 +750,7 @@ __device__ void vcycle_levels(const LevDesc* __restrict__ levTab, int ns, int s,
     const LevDesc& A = LEV(l, s);
     const LevDesc& C = LEV(l + 1, s);
     smooth_dom(A, pre, d);
-    for (int p = d.tid; p < A.n; p += d.nth) res_row32(A, p);
-    d.sync();
-    for (int P = d.tid; P < C.n; P += d.nth) restrict_row32(A, C, P);
+    for (int P = d.tid; P < C.n; P += d.nth) restrict_res_row32(A, C, P);
     d.sync();
   }
   coarse_apply(LEV(L, s), cinv + (size_t)s * kDense * kDense, d);
@@ -1242,7 +1264,7 @@ int Service::solve_u(bool g) {
   UFVM_LAUNCH_CHECK();
   auto body = [&]() -> int {
     for (int pass = 0; pass < 2; ++pass)
-      for (int q = 0; q < ucolors; ++q) {
+      for (int q = pass; q < ucolors; ++q) {  // the backward pass skips the repeated colour
         const int c = pass == 0 ? q : ucolors - 1 - q;
         if (ucol_cnt[c] == 0) continue;
         if (u_items) k_mc64_items<<<ucol_cnt[c], kBlock, 0, stream>>>(wu_items.p + ucol_off[c], uctl.p);
@@ -1299,7 +1321,7 @@ int Service::solve_p(bool g) {
   auto smooth = [&](int l, int sweeps) {
     for (int k = 0; k < sweeps; ++k)
       for (int pass = 0; pass < 2; ++pass)
-        for (int q = 0; q < maxcol[l]; ++q) {
+        for (int q = pass; q < maxcol[l]; ++q) {  // the backward pass skips the repeated colour
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
           if (l == 0 && l0_items) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(wsm0.p + smoff[0][c], pctl.p);
@@ -1633,8 +1655,9 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
 // and returns the average device time of one unit and its compulsory bytes (every array
 // touched once per pass; neighbour gathers of x counted as cache hits). Units:
 //   0: one symmetric FP64 multicolour Gauss-Seidel sweep of every slot's level 0 (k_mc64 on
-//      the ELL copy, 2 x colours launches): 2 x (32 B per row -- ac, bc, x written, x read
-//      once -- + 12 B per nonzero);
+//      the ELL copy, 2 x colours - 1 launches): 2 x (32 B per row -- ac, bc, x written, x read
+//      once -- + 12 B per nonzero), less the rows of the last colour, which the backward pass
+//      skips;
 //   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32, colour-permuted ELL):
 //      2 x (16 B per row -- ac, bc, x written, x read once -- + 8 B per nonzero);
 //   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz;
@@ -1665,7 +1688,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   auto unit = [&]() -> int {
     if (kernel == 0) {
       for (int pass = 0; pass < 2; ++pass)
-        for (int q = 0; q < ucolors; ++q) {
+        for (int q = pass; q < ucolors; ++q) {
           const int c = pass == 0 ? q : ucolors - 1 - q;
           if (ucol_cnt[c] == 0) continue;
           if (u_items) k_mc64_items<<<ucol_cnt[c], kBlock, 0, stream>>>(wu_items.p + ucol_off[c], uctl.p);
@@ -1674,7 +1697,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
         }
     } else if (kernel == 1) {
       for (int pass = 0; pass < 2; ++pass)
-        for (int q = 0; q < maxcol[0]; ++q) {
+        for (int q = pass; q < maxcol[0]; ++q) {
           const int c = pass == 0 ? q : maxcol[0] - 1 - q;
           if (smcnt[0][c] == 0) continue;
           if (l0_items) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(wsm0.p + smoff[0][c], pctl.p);
@@ -1729,8 +1752,21 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   *ms = t / reps;
   double Fi = 0, F = 0, R = 0;
   for (auto* c : cases) { Fi += c->M.Fi; F += c->M.F; R += c->M.Nc + c->M.Fb; }
-  if (kernel == 0) *bytes = 2.0 * (32.0 * N + 12.0 * NNZ);
-  else if (kernel == 1) *bytes = 2.0 * (16.0 * N + 8.0 * NNZ);
+  // rows of the last colour that the backward pass skips (slots with the most colours only)
+  double skipN = 0, skipNNZ = 0;
+  if (kernel <= 1) {
+    const int C = kernel == 0 ? ucolors : maxcol[0];
+    for (auto* c : cases) {
+      const Level& L0 = c->lev[0];
+      if (!L0.color_valid || L0.ncolor != C || (int)L0.h_colorStart.size() <= C) continue;
+      if (kernel == 1 && !(c->hierarchy_valid && c->n_levels > 1)) continue;
+      const double last = (double)(L0.h_colorStart[C] - L0.h_colorStart[C - 1]);
+      skipN += last;
+      skipNNZ += (double)c->M.nnz * last / (double)c->M.Nc;
+    }
+  }
+  if (kernel == 0) *bytes = 2.0 * (32.0 * N + 12.0 * NNZ) - (32.0 * skipN + 12.0 * skipNNZ);
+  else if (kernel == 1) *bytes = 2.0 * (16.0 * N + 8.0 * NNZ) - (16.0 * skipN + 8.0 * skipNNZ);
   else if (kernel == 2) *bytes = 36.0 * N + 12.0 * NNZ;
   else if (kernel == 3) *bytes = 48.0 * N + 80.0 * Fi;
   else if (kernel == 4) *bytes = 96.0 * N + 120.0 * Fi;

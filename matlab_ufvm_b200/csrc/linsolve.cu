@@ -1051,8 +1051,10 @@ int mcgs_sweep(LinCtx& c, Level& L) {
   // the first colour kernel of the sweep waits for all earlier work the ordinary way; the
   // later ones are programmatic dependents of the colour before them
   int launched = 0;
+  // the backward pass starts one colour in: its first colour would repeat the forward pass's
+  // last update from the same neighbour values (same bits), so it is skipped
   for (int pass = 0; pass < 2; ++pass) {
-    for (int q = 0; q < L.ncolor; ++q) {
+    for (int q = pass; q < L.ncolor; ++q) {
       const int col_ = pass == 0 ? q : L.ncolor - 1 - q;
       const int s = L.h_colorStart[col_], cnt = L.h_colorStart[col_ + 1] - s;
       if (cnt <= 0) continue;
