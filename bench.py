@@ -796,7 +796,8 @@ def main_ours(args):
                "h2d_bytes_per_step": int(reduce_sum(r2["h2d"], ws) / args.steps),
                "d2h_bytes_per_step": int(reduce_sum(r2["d2h"], ws) / args.steps),
                "wall_s": round(r2["wall"], 3), "device_s": round(r2["ms"] * 1e-3, 3),
-               "complete": bool(r2["complete"])}
+               "device_s_in_ticks": round(sum(b["ms"] for b in r2["tail"]) * 1e-3, 3),
+               "first_tick_ms": r2["first_tick_ms"], "complete": bool(r2["complete"])}
     plain = cpu = check = None
     if rank == 0 and ws == 1:
         fix = oracle_fixture() if os.path.exists(ORACLE_FIXTURE) else None

@@ -18,7 +18,9 @@
 // A step without hierarchy builds is captured once and replayed as a CUDA graph whose solve
 // loops are conditional WHILE nodes ended on the device.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <thread>
 
 #include "fast.cuh"
 
@@ -1083,14 +1085,72 @@ BatchLaunch Service::batch() {
 }
 
 // The reference's agglomeration of the assembled p matrix, FP32 arrays and colourings.
-int Service::ensure_hierarchy(Case& c) {
+int Service::ensure_hierarchy(Case& c, cudaStream_t st) {
   const long long b0 = t_dev_bytes;
-  const int st = ensure_hierarchy_(c);
+  cudaStream_t own = c.lin.stream;
+  c.lin.stream = st;  // the case's scratch and solver work run on `st` for the build
+  const int rc = ensure_hierarchy_(c, st);
+  c.lin.stream = own;
   c.dev_bytes += t_dev_bytes - b0;
-  return st;
+  return rc;
 }
 
-int Service::ensure_hierarchy_(Case& c) {
+// Hierarchy builds of several newly admitted cases: each case's build is a chain of small
+// launches and host waits (agglomeration rounds, colourings, the host-side ELL permutation), and
+// the cases are independent, so they run on up to kBuildThreads host threads, each with its own
+// stream, after the assembly that produced their matrices; the service stream then waits for all
+// of them. A build's result does not depend on which thread or stream ran it.
+int Service::build_hierarchies(std::vector<Case*>& need) {
+  if (need.empty()) return UFVM_OK;
+  const int nt = (int)std::min<size_t>(need.size(), kBuildThreads);
+  if (nt <= 1) {
+    for (Case* c : need) UFVM_CHECK(ensure_hierarchy(*c, stream));
+    return UFVM_OK;
+  }
+  int dev = 0;
+  UFVM_CUDA(cudaGetDevice(&dev));
+  while ((int)build_streams.size() < nt) {
+    cudaStream_t s2 = nullptr;
+    UFVM_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    build_streams.push_back(s2);
+  }
+  if (!build_event) UFVM_CUDA(cudaEventCreateWithFlags(&build_event, cudaEventDisableTiming));
+  UFVM_CUDA(cudaEventRecord(build_event, stream));
+  std::atomic<size_t> next{0};
+  std::vector<int> rc(nt, UFVM_OK);
+  std::vector<std::string> msg(nt);
+  auto worker = [&](int w) {
+    if (cudaSetDevice(dev) != cudaSuccess || cudaStreamWaitEvent(build_streams[w], build_event, 0) != cudaSuccess) {
+      rc[w] = UFVM_E_CUDA;
+      msg[w] = "a hierarchy build thread could not join the service's device or stream";
+      return;
+    }
+    for (size_t k = next++; k < need.size(); k = next++) {
+      const int r = ensure_hierarchy(*need[k], build_streams[w]);
+      if (r != UFVM_OK) {
+        rc[w] = r;
+        msg[w] = get_error();
+        return;
+      }
+    }
+    if (cudaStreamSynchronize(build_streams[w]) != cudaSuccess) {
+      rc[w] = UFVM_E_CUDA;
+      msg[w] = "hierarchy build stream failed";
+    }
+  };
+  std::vector<std::thread> th;
+  for (int w = 1; w < nt; ++w) th.emplace_back(worker, w);
+  worker(0);
+  for (auto& t : th) t.join();
+  for (int w = 0; w < nt; ++w)
+    if (rc[w] != UFVM_OK) {
+      set_error(msg[w]);
+      return rc[w];
+    }
+  return UFVM_OK;
+}
+
+int Service::ensure_hierarchy_(Case& c, cudaStream_t st) {
   c.amg->smoother = UFVM_SMOOTHER_MCGS; c.amg->quirks = c.S.quirks;
   UFVM_CHECK(c.amg->build(c.lev, c.S.p_max_coarse_levels, c.S.quirks, &c.n_levels));
   for (int l = 0; l < c.n_levels; ++l) {
@@ -1107,9 +1167,8 @@ int Service::ensure_hierarchy_(Case& c) {
       UFVM_CHECK(dalloc(L.fq, L.n));
     }
   }
-  if (c.n_levels > 1) UFVM_CHECK(build_ell(c));
+  if (c.n_levels > 1) UFVM_CHECK(build_ell(c, st));
   c.hierarchy_valid = true;
-  tables_dirty = true;
   return UFVM_OK;
 }
 
@@ -1154,7 +1213,7 @@ int Service::loop_end() {
 // Every level but the coarsest of the FP32 V-cycle in colour-permuted ELL form (built once
 // per hierarchy): rows sorted by colour, natural order inside a colour (a stable counting
 // sort on the host).
-int Service::build_ell(Case& c) {
+int Service::build_ell(Case& c, cudaStream_t st) {
   const int nl = c.n_levels;
   if (nl < 2) return UFVM_OK;
   std::vector<std::vector<int>> perm(nl), inv(nl);
@@ -1164,8 +1223,8 @@ int Service::build_ell(Case& c) {
     if (!L.color_valid) { set_error("build_ell: level without a colouring"); return UFVM_E_INVALID; }
     const int n = L.n;
     std::vector<int> color(n);
-    UFVM_CUDA(cudaMemcpyAsync(color.data(), L.color.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    UFVM_CUDA(cudaStreamSynchronize(stream));
+    UFVM_CUDA(cudaMemcpyAsync(color.data(), L.color.p, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFVM_CUDA(cudaStreamSynchronize(st));
     std::vector<int> start(L.ncolor + 1, 0);
     for (int i = 0; i < n; ++i) {
       if (color[i] < 0 || color[i] >= L.ncolor) { set_error("build_ell: row without a colour"); return UFVM_E_INVALID; }
@@ -1186,12 +1245,12 @@ int Service::build_ell(Case& c) {
     const bool cperm = l + 2 < nl;  // the next level is permuted too (it is not the coarsest)
     const int n = L.n, nnz = L.nnz, nc = C.n;
     std::vector<int> rp(n + 1), col(std::max(nnz, 1)), parents(n), cs(nc + 1), child(n);
-    UFVM_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    if (nnz) UFVM_CUDA(cudaMemcpyAsync(col.data(), L.col.p, nnz * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    UFVM_CUDA(cudaMemcpyAsync(parents.data(), L.parents.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    UFVM_CUDA(cudaMemcpyAsync(cs.data(), L.childStart.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    UFVM_CUDA(cudaMemcpyAsync(child.data(), L.child.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    UFVM_CUDA(cudaStreamSynchronize(stream));
+    UFVM_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (nnz) UFVM_CUDA(cudaMemcpyAsync(col.data(), L.col.p, nnz * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFVM_CUDA(cudaMemcpyAsync(parents.data(), L.parents.p, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFVM_CUDA(cudaMemcpyAsync(cs.data(), L.childStart.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFVM_CUDA(cudaMemcpyAsync(child.data(), L.child.p, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFVM_CUDA(cudaStreamSynchronize(st));
     const std::vector<int>& P = perm[l];
     const std::vector<int>& I = inv[l];
     int W = 0;
@@ -1209,18 +1268,18 @@ int Service::build_ell(Case& c) {
       chS[Q + 1] = (int)chP.size();
     }
     if ((int)chP.size() != n) { set_error("build_ell: children do not cover the level"); return UFVM_E_INVALID; }
-    UFVM_CHECK(upload_vec(L.perm, P, stream));
-    UFVM_CHECK(upload_vec(L.inv, I, stream));
-    UFVM_CHECK(upload_vec(L.ellCol, ell, stream));
-    UFVM_CHECK(upload_vec(L.parentsP, parP, stream));
-    UFVM_CHECK(upload_vec(L.childP, chP, stream));
-    UFVM_CHECK(upload_vec(L.childStartP, chS, stream));
+    UFVM_CHECK(upload_vec(L.perm, P, st));
+    UFVM_CHECK(upload_vec(L.inv, I, st));
+    UFVM_CHECK(upload_vec(L.ellCol, ell, st));
+    UFVM_CHECK(upload_vec(L.parentsP, parP, st));
+    UFVM_CHECK(upload_vec(L.childP, chP, st));
+    UFVM_CHECK(upload_vec(L.childStartP, chS, st));
     {  // Galerkin target of every fine entry: -1 inside the aggregate, else the coarse position
       std::vector<int> crp(nc + 1), ccol(std::max(C.nnz, 1));
-      UFVM_CUDA(cudaMemcpyAsync(crp.data(), C.rowptr.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      UFVM_CUDA(cudaMemcpyAsync(crp.data(), C.rowptr.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
       if (C.nnz)
-        UFVM_CUDA(cudaMemcpyAsync(ccol.data(), C.col.p, C.nnz * sizeof(int), cudaMemcpyDeviceToHost, stream));
-      UFVM_CUDA(cudaStreamSynchronize(stream));
+        UFVM_CUDA(cudaMemcpyAsync(ccol.data(), C.col.p, C.nnz * sizeof(int), cudaMemcpyDeviceToHost, st));
+      UFVM_CUDA(cudaStreamSynchronize(st));
       std::vector<int> gp(std::max(nnz, 1), -2);
       for (int i = 0; i < n; ++i) {
         const int Pi = parents[i];
@@ -1231,7 +1290,7 @@ int Service::build_ell(Case& c) {
             if (ccol[t] == Q) { gp[k] = t; break; }
         }
       }
-      UFVM_CHECK(upload_vec(L.gpos, gp, stream));
+      UFVM_CHECK(upload_vec(L.gpos, gp, st));
     }
     UFVM_CHECK(dalloc(L.ellAnb, std::max<size_t>((size_t)W * n, 1)));
     if (l == 0) {  // FP64 ELL copy of the momentum matrix for the U solve
@@ -1240,7 +1299,7 @@ int Service::build_ell(Case& c) {
       UFVM_CHECK(dalloc(L.uBc, n));
       UFVM_CHECK(dalloc(L.uX, n));
     }
-    UFVM_CUDA(cudaStreamSynchronize(stream));  // the host vectors above go out of scope
+    UFVM_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
     L.ellW = W;
     L.ell_valid = true;
   }
@@ -1429,12 +1488,14 @@ int Service::enqueue_tick(bool g, std::vector<std::pair<int, int>>& marks) {
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_MAX, SCAL_P_MAX);
     UFVM_CHECK(mark(PH_HIER));
     if (!g) {
-      bool built = false;
+      std::vector<Case*> need;
       for (auto* c : cases) {
-        if (needs_hierarchy(*c)) { UFVM_CHECK(ensure_hierarchy(*c)); built = true; }
+        if (needs_hierarchy(*c)) need.push_back(c);
         c->p_solves++;
       }
-      if (built) {
+      UFVM_CHECK(build_hierarchies(need));
+      if (!need.empty()) {
+        tables_dirty = true;
         UFVM_CHECK(rebuild_tables());
         b = batch();
       }
@@ -1796,6 +1857,10 @@ Service::~Service() {
   if (graph) destroy_check(cudaGraphDestroy(graph), "cudaGraphDestroy");
   gexec = nullptr;
   graph = nullptr;
+  for (cudaStream_t bs : build_streams) destroy_check(cudaStreamDestroy(bs), "cudaStreamDestroy");
+  build_streams.clear();
+  if (build_event) destroy_check(cudaEventDestroy(build_event), "cudaEventDestroy");
+  build_event = nullptr;
   for (auto* c : cases) delete c;
   cases.clear();
   for (auto* a : {&scal, &part, &fcg}) dfree(*a);

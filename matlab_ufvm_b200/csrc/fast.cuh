@@ -30,6 +30,7 @@ struct LevDesc {
 // Packed coarse V-cycle: CTAs of kBlockPack threads; a task gives one large case the whole
 // CTA or each of kPackGroups thread groups its own small case (slot -1: none).
 constexpr int kBlockPack = 1024;
+constexpr size_t kBuildThreads = 8;  // host threads that build new cases' AMG hierarchies
 constexpr int kPackGroups = 4;
 struct PackTask {
   int big;
@@ -147,9 +148,12 @@ struct Service {
   int rebuild_tables();
   BatchLaunch batch();
   bool needs_hierarchy(const Case& c) const;
-  int ensure_hierarchy(Case& c);   // adds the bytes it allocates to c.dev_bytes
-  int ensure_hierarchy_(Case& c);
-  int build_ell(Case& c);
+  int ensure_hierarchy(Case& c, cudaStream_t st);  // adds the bytes it allocates to c.dev_bytes
+  int ensure_hierarchy_(Case& c, cudaStream_t st);
+  int build_hierarchies(std::vector<Case*>& need);
+  int build_ell(Case& c, cudaStream_t st);
+  std::vector<cudaStream_t> build_streams;  // streams of the hierarchy-build threads
+  cudaEvent_t build_event = nullptr;
   int loop_begin(int kind, cudaGraphConditionalHandle* h);
   int loop_end();
   int solve_u(bool g);
