@@ -325,6 +325,7 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                host_ms={k: round(s1[k] - s0[k], 1) for k in ("host_rebuild_ms", "host_capture_ms", "host_drop_ms")},
                peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
                tickets=tickets, tail=tail_profile(tick_log, len(specs)), admit_s=admit_s,
+               cta_rows=s1["cta_rows"], tunes=s1["tunes"],
                first_tick_ms=tick_log[0][1] if tick_log else None)
     return svc, out
 
@@ -797,7 +798,8 @@ def main_ours(args):
                "d2h_bytes_per_step": int(reduce_sum(r2["d2h"], ws) / args.steps),
                "wall_s": round(r2["wall"], 3), "device_s": round(r2["ms"] * 1e-3, 3),
                "device_s_in_ticks": round(sum(b["ms"] for b in r2["tail"]) * 1e-3, 3),
-               "first_tick_ms": r2["first_tick_ms"], "complete": bool(r2["complete"])}
+               "first_tick_ms": r2["first_tick_ms"], "complete": bool(r2["complete"]),
+               "ticks_by_active_cases": r2["tail"], "cta_rows": r2["cta_rows"]}
     plain = cpu = check = None
     if rank == 0 and ws == 1:
         fix = oracle_fixture() if os.path.exists(ORACLE_FIXTURE) else None
@@ -833,7 +835,7 @@ def main_ours(args):
             "ticks_by_active_cases": res["tail"], "host_ms_in_timed_region": res["host_ms"],
             "device_ms_in_ticks": round(sum(b["ms"] for b in res["tail"]), 1),
             "admission_s_before_timing": round(res["admit_s"], 3) if res["admit_s"] is not None else None,
-            "first_tick_ms": res["first_tick_ms"],
+            "first_tick_ms": res["first_tick_ms"], "cta_rows": res["cta_rows"],
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res["clocks"],
         }
         if cpu:

@@ -9,18 +9,22 @@ iterated to its fixed point, with the distance from that fixed point of the orac
 the reference's residualControl test (booleans/cfdCheckConvergence.m:3-20, residuals as
 compute/cfdComputeNormalizedResidual.m:27-88) first passes at each tolerance.
 
-All pinned cases run together in one service (FP64 multicolour Gauss-Seidel for U, FP32
-agglomeration AMG preconditioning FP64 flexible CG for p), to the tight tolerance TIGHT, and the
+The pinned cases run in the service (FP64 multicolour Gauss-Seidel for U, FP32 agglomeration
+AMG preconditioning FP64 flexible CG for p) to the tightest residualControl the oracle itself
+reached on the case (1e-11 on all but one, which stagnates at 1.3e-11 and gets 1e-10), and the
 fields are also read at the tick where the residuals first pass 1e-6 -- the iterate at which the
 bench's runs stop. Field error is the relative L2 distance of U (all three components over the
-cells) and of p - p[cell 0] from the oracle's fixed point.
+cells) and of p - p[cell 0] from the oracle's fixed point (its last iterate, stored in float32:
+about 6e-8 of rounding).
 
-Checked, per case:
+At a residual of 1e-6 a SIMPLE iterate is far from the fixed point: the oracle's own fields are
+6e-6 to 2e-2 away (the error falls ten times per decade of residual, so the large meshes need a
+residual near 1e-11 for 1e-6). Checked, per case:
 * at the 1e-6 stop, the service's field error is of the same size as the oracle's own at its
-  1e-6 stop (both are a few hundred times the residual; at most 4x the oracle's);
+  1e-6 stop (at most SAME_SIZE times it);
 * for n <= 128, the service's 1e-6 fields against the oracle's 1e-6 fields (the same stopping
-  rule on both sides) differ by less than the larger of the two stops' errors;
-* at TIGHT, the service's field error is <= 1e-6.
+  rule on both sides) differ by less than the sum of the two stops' errors;
+* at the tight stop, the service's field error is <= 1e-6.
 """
 import json
 import os
@@ -35,8 +39,7 @@ pytestmark = pytest.mark.gpu
 
 FIXTURE = os.path.join(GOLDEN, "sweep_oracle.json")
 FIELDS = os.path.join(GOLDEN, "sweep_oracle_fields.npz")
-TIGHT = 1e-9          # residualControl of the tight run
-FIELD_TOL = 1e-6      # field error allowed at TIGHT
+FIELD_TOL = 1e-6      # field error allowed at the tight stop
 SAME_SIZE = 4.0       # service error at the 1e-6 stop <= this x the oracle's own
 
 
@@ -52,7 +55,7 @@ def run_pinned(ufvm, cases, fields, tol):
     specs = [case.cavity_case(c["n"], nu=1.0 / c["re"], quirks=case.QUIRKS_CONVERGING, tol_u=tol, tol_p=tol)
              for c in cases]
     svc = ufvm.Service(ufvm.fast_settings(specs[0]))
-    tickets = [svc.submit(s, 40000) for s in specs]
+    tickets = [svc.submit(s, 60000) for s in specs]
     at6 = {}
     done = set()
     while len(done) < len(tickets):
@@ -82,11 +85,21 @@ def _perr(p, pref):
     return rel(p - p[0], pref - pref[0])
 
 
+def tight_tol(c):
+    """The tightest residual decade the oracle reached on this case."""
+    return 10.0 ** -max(int(k) for k in c["first"])
+
+
 def test_service_at_operating_point_against_oracle(ufvm_mod):
     cases = _pinned()
     assert len(cases) >= 12
     z = np.load(FIELDS)
-    res = run_pinned(ufvm_mod, cases, z, TIGHT)
+    results = {}
+    for tol in sorted({tight_tol(c) for c in cases}):
+        group = [c for c in cases if tight_tol(c) == tol]
+        for c, r in zip(group, run_pinned(ufvm_mod, group, z, tol)):
+            results[c["index"]] = r
+    res = [results[c["index"]] for c in cases]
     report = []
     for c, r in zip(cases, res):
         i = c["index"]
@@ -96,7 +109,7 @@ def test_service_at_operating_point_against_oracle(ufvm_mod):
                "service_it_1e-6": r["it6"], "oracle_it_1e-6": c["first"]["6"],
                "service_err_u_1e-6": rel(r["U6"], Uf), "service_err_p_1e-6": _perr(r["p6"], pf),
                "oracle_err_u_1e-6": c["err_u"]["6"], "oracle_err_p_1e-6": c["err_p"]["6"],
-               "service_it_tight": r["it"], "service_err_u_tight": rel(r["U"], Uf),
+               "tight_tol": tight_tol(c), "service_it_tight": r["it"], "service_err_u_tight": rel(r["U"], Uf),
                "service_err_p_tight": _perr(r["p"], pf)}
         if f"U_6_{i}" in z.files:
             row["same_rule_u"] = rel(r["U6"], z[f"U_6_{i}"].astype(np.float64))
@@ -105,12 +118,12 @@ def test_service_at_operating_point_against_oracle(ufvm_mod):
     path = os.environ.get("UFVM_OPERATING_POINT_REPORT")
     if path:
         with open(path, "w") as f:
-            json.dump({"tight": TIGHT, "cases": report}, f, indent=1)
+            json.dump({"cases": report}, f, indent=1)
     for row in report:
         what = f"n={row['n']} Re={row['re']}"
         assert row["service_err_u_tight"] <= FIELD_TOL and row["service_err_p_tight"] <= FIELD_TOL, (what, row)
         assert row["service_err_u_1e-6"] <= SAME_SIZE * row["oracle_err_u_1e-6"] + FIELD_TOL, (what, row)
         assert row["service_err_p_1e-6"] <= SAME_SIZE * row["oracle_err_p_1e-6"] + FIELD_TOL, (what, row)
         if "same_rule_u" in row:
-            bound = max(row["service_err_u_1e-6"], row["oracle_err_u_1e-6"]) + FIELD_TOL
-            assert row["same_rule_u"] <= bound, (what, row)
+            assert row["same_rule_u"] <= row["service_err_u_1e-6"] + row["oracle_err_u_1e-6"] + FIELD_TOL, (what, row)
+            assert row["same_rule_p"] <= row["service_err_p_1e-6"] + row["oracle_err_p_1e-6"] + FIELD_TOL, (what, row)
