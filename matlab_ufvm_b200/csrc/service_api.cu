@@ -21,7 +21,9 @@
 #include <map>
 #include <memory>
 
+#include <atomic>
 #include <chrono>
+#include <thread>
 
 #include "fast.cuh"
 
@@ -201,10 +203,108 @@ static bool admission_due(const ServiceImpl& S) {
   return S.resident_cells == 0 || S.steps_since_admit >= S.admit_interval || 2 * S.resident_cells <= S.max_cells;
 }
 
+// A case created ahead of the admission loop (by precreate below).
+struct Precreated {
+  Case* c = nullptr;
+  int status = UFVM_OK;
+  long long bytes = 0;
+  std::string err;
+};
+
+static void case_settings(const ServiceImpl& S, const Pending& p, ufvm_settings& cs) {
+  cs = S.svc.S;
+  cs.nu = p.nu;
+  // the pressure reference cell is per case, as in cfdReadSystem.m:238-252: a case whose
+  // boundaries are all walls, empty or symmetry planes pins p at the settings' pRefCell
+  // (cell 0 when the shared settings carry none); any other case has no reference cell
+  bool closed = true;
+  for (int32_t t : p.ptype)
+    if (t != UFVM_PATCH_WALL && t != UFVM_PATCH_EMPTY && t != UFVM_PATCH_SYMMETRY) closed = false;
+  cs.fixed_element = closed ? std::max(0, S.svc.S.fixed_element) : -1;
+}
+
+// Creating a case (mesh connectivity on the host, uploads, geometry kernels, a wait for them) is
+// independent from case to case, so when several queued cases are about to be admitted they are
+// created ahead on up to kBuildThreads host threads, each on its own stream, and the admission
+// loop below takes them in queue order. The queue prefix is the one the loop would admit by the
+// same checks (estimated bytes and cells); a case the loop does not take is freed again. A
+// created case then runs on the service stream like any other.
+static std::map<long long, Precreated> precreate(ServiceImpl& S) {
+  std::map<long long, Precreated> out;
+  std::vector<Pending*> pick;
+  long long cells = S.resident_cells, bytes = S.slot_bytes() + S.snap_bytes, est_sum = 0;
+  bool empty = S.svc.cases.empty();
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return out;
+  }
+  for (Pending& p : S.queue) {
+    const long long est = S.estimate(p.est_raw);
+    if (!empty && (cells + p.cells > S.max_cells || bytes + est > S.max_bytes)) break;
+    if (est_sum + est + (est >> 3) > (long long)fr) break;
+    cells += p.cells;
+    bytes += est;
+    est_sum += est;
+    empty = false;
+    pick.push_back(&p);
+  }
+  if (pick.size() < 4) return out;  // a few cases: the loop creates them itself
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return out;
+  }
+  const int nt = (int)std::min<size_t>(pick.size(), kBuildThreads);
+  std::vector<Precreated> res(pick.size());
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    cudaStream_t st = nullptr;
+    if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return;  // the cases this thread would have made are created by the loop instead
+    }
+    for (size_t k = next++; k < pick.size(); k = next++) {
+      const Pending& p = *pick[k];
+      ufvm_mesh_desc d;
+      fill_desc(p, d);
+      ufvm_settings cs;
+      case_settings(S, p, cs);
+      Case* c = new Case();
+      const long long b0 = t_dev_bytes;
+      const int rc = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr,
+                                      nullptr, nullptr, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) cudaGetLastError();
+      res[k].bytes = t_dev_bytes - b0;
+      res[k].status = rc;
+      if (rc != UFVM_OK) res[k].err = get_error();
+      c->stream = S.svc.stream;  // from here on the case runs on the service stream
+      c->lin.stream = S.svc.stream;
+      res[k].c = c;
+    }
+    cudaStreamDestroy(st);
+  };
+  std::vector<std::thread> th;
+  for (int w = 1; w < nt; ++w) th.emplace_back(worker);
+  worker();
+  for (auto& t : th) t.join();
+  for (size_t k = 0; k < pick.size(); ++k)
+    if (res[k].c) out[pick[k]->ticket] = res[k];
+  return out;
+}
+
 static int admit(ServiceImpl& S) {
   if (!admission_due(S)) return UFVM_OK;
   drop_frozen(S);  // departures are gathered into the admission's table rebuild
   const size_t before = S.svc.cases.size();
+  std::map<long long, Precreated> pre = precreate(S);
+  auto take_pre = [&](long long ticket, Precreated& out) -> bool {
+    auto it = pre.find(ticket);
+    if (it == pre.end()) return false;
+    out = it->second;
+    pre.erase(it);
+    return true;
+  };
   while (!S.queue.empty()) {
     Pending& p = S.queue.front();
     const long long est = S.estimate(p.est_raw);
@@ -223,30 +323,33 @@ static int admit(ServiceImpl& S) {
     }
     ufvm_mesh_desc d;
     fill_desc(p, d);
-    ufvm_settings cs = S.svc.S;
-    cs.nu = p.nu;
-    // the pressure reference cell is per case, as in cfdReadSystem.m:238-252: a case whose
-    // boundaries are all walls, empty or symmetry planes pins p at the settings' pRefCell
-    // (cell 0 when the shared settings carry none); any other case has no reference cell
-    bool closed = true;
-    for (int32_t t : p.ptype)
-      if (t != UFVM_PATCH_WALL && t != UFVM_PATCH_EMPTY && t != UFVM_PATCH_SYMMETRY) closed = false;
-    cs.fixed_element = closed ? std::max(0, S.svc.S.fixed_element) : -1;
-    Case* c = new Case();
-    const long long b0 = t_dev_bytes;
+    ufvm_settings cs;
+    case_settings(S, p, cs);
+    Case* c = nullptr;
     int st;
     bool injected = false;
+    Precreated made;
+    const bool premade = take_pre(p.ticket, made);
     auto inj = S.inject_oom.find(p.ticket);
     if (inj != S.inject_oom.end() && inj->second > 0) {  // a failed device allocation, injected
       --inj->second;
+      if (premade) delete made.c;
+      c = new Case();
       set_error("cudaMalloc: out of memory (injected)");
       st = UFVM_E_OOM;
       injected = true;
+    } else if (premade) {
+      c = made.c;
+      st = made.status;
+      c->dev_bytes = made.bytes;
+      if (st != UFVM_OK) set_error(made.err);
     } else {
+      c = new Case();
+      const long long b0 = t_dev_bytes;
       st = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr, nullptr,
                             nullptr, S.svc.stream);
+      c->dev_bytes = t_dev_bytes - b0;
     }
-    c->dev_bytes = t_dev_bytes - b0;
     Record& r = S.rec[p.ticket];
     if (st == UFVM_E_OOM && !injected && !S.graveyard.empty()) {  // room held by departed cases: free it, retry
       delete c;
@@ -285,6 +388,7 @@ static int admit(ServiceImpl& S) {
     S.svc.tables_dirty = true;
     S.queue.pop_front();
   }
+  for (auto& kv : pre) delete kv.second.c;  // created ahead but not admitted this time
   if (S.svc.cases.size() != before) S.steps_since_admit = 0;
   return UFVM_OK;
 }
@@ -396,6 +500,19 @@ int ufvm_service_create(const ufvm_settings* settings, int64_t max_resident_cell
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&S.svc.nsm, cudaDevAttrMultiProcessorCount, dev);
   S.svc.lin.stream = S.svc.stream;
+  // Result snapshots come from the device's default memory pool (stream-ordered, no device
+  // synchronisation); the pool keeps what released results give back for the next ones instead
+  // of returning it to the driver at every synchronisation, which would unmap and map memory
+  // between steps.
+  {
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) cudaGetLastError();
+    } else {
+      cudaGetLastError();
+    }
+  }
   // default HBM budget: 90% of the device memory free when the service starts
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
