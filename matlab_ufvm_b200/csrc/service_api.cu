@@ -26,6 +26,7 @@
 #include <thread>
 
 #include "fast.cuh"
+#include "linsolve.cuh"
 
 namespace ufvm {
 
@@ -272,8 +273,12 @@ static std::map<long long, Precreated> precreate(ServiceImpl& S) {
       case_settings(S, p, cs);
       Case* c = new Case();
       const long long b0 = t_dev_bytes;
-      const int rc = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr,
-                                      nullptr, nullptr, st);
+      int rc = create_case_into(*c, &d, cs, p.bcu.data(), p.bcp.data(), p.bvu.data(), p.bvp.data(), nullptr,
+                                nullptr, nullptr, st);
+      // the level-0 system and its colouring depend on the mesh only: made here too, in parallel,
+      // instead of one case after another in the first step
+      if (rc == UFVM_OK) rc = c->fresh_level0();
+      if (rc == UFVM_OK) rc = build_coloring(c->lin, c->lev[0]);
       if (cudaStreamSynchronize(st) != cudaSuccess) cudaGetLastError();
       res[k].bytes = t_dev_bytes - b0;
       res[k].status = rc;
