@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--workload", choices=("sweep", "serving"), default="sweep",
                     help="sweep: the 512-case 2D cavity batch (the headline line); serving: the Poisson-arrival "
                          "mix of 2D/3D cavities and tet channels (its own JSON line)")
-    ap.add_argument("--serving-requests", type=int, default=48, help="requests per serving phase")
+    ap.add_argument("--serving-requests", type=int, default=96, help="requests per serving phase")
     ap.add_argument("--capacity-steps", type=int, default=400, help="service steps of the closed-loop phase")
     ap.add_argument("--serving-max-iter", type=int, default=8000,
                     help="SIMPLE iteration limit of a serving request (the case script's endTime)")
