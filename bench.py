@@ -347,6 +347,13 @@ def tail_profile(tick_log, cases):
 ROOF_KERNEL = (1, "k_mc32_l0 (FP32 multicolour Gauss-Seidel sweep of the V-cycle's level 0, "
                   "colour-permuted ELL; one unit = both colours forward then backward over every case)")
 
+# DRAM traffic per byte of the bytes model, from one ncu capture of each unit's kernels on a
+# 160-case batch (profiles/k_uface_k_assemble_u_cavity_batch.md: k_uface + k_assemble_u moved
+# 1534.5 MB against 341.9 MB of the model; profiles/k_mc32_level0_cavity_sweep.md: 176.4 MB
+# against 188.3 MB). Traffic grows in proportion to the batch, so the live unit's traffic is
+# this ratio times its model bytes.
+TRAFFIC_PER_MODEL_BYTE = {3: 1534.5 / 341.9, 1: 176.4 / 188.3}
+
 # Units of the service's profiling hook: (id, name, units per tick as a function of the tick's U
 # smoother sweeps and p V-cycles, bound)
 TICK_UNITS = (
@@ -446,8 +453,14 @@ def roofline(svc, peaks, ticks: int = 12):
                      "share_of_tick": round(t / tick_ms, 4) if tick_ms > 0 else None})
     top = max(rows, key=lambda r: r["ms_per_tick"])
     top_hbm = max((r for r in rows if r["bound"] == "hbm"), key=lambda r: r["ms_per_tick"])
+    top_id = next(kid for kid, name, _, _ in TICK_UNITS if name == top_hbm["kernel"])
+    ratio = TRAFFIC_PER_MODEL_BYTE.get(top_id)
+    traffic = round(ratio * top_hbm["bytes_per_unit"]) if ratio else None
     return {"kernel": top_hbm["kernel"], "bound": "hbm", "achieved": top_hbm["achieved"], "peak": peak,
-            "unit": "GB/s", "frac": top_hbm["frac"], "traffic": None, "bytes_per_unit": top_hbm["bytes_per_unit"],
+            "unit": "GB/s", "frac": top_hbm["frac"], "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on a 160-case batch, scaled to this "
+                              "batch by the bytes model" if traffic else None,
+            "bytes_per_unit": top_hbm["bytes_per_unit"],
             "ms_per_unit": top_hbm["ms_per_unit"], "share_of_tick": top_hbm["share_of_tick"],
             "largest_kernel_of_tick": top["kernel"],
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if not peaks.get("fallback")
