@@ -152,6 +152,8 @@ def main():
     ap.add_argument("--workers", type=int, default=max(1, (os.cpu_count() or 2) - 1))
     ap.add_argument("--parts", default=os.path.join(tempfile.gettempdir(), "ufvm_sweep_oracle_parts"))
     ap.add_argument("--variant", choices=("reference", "plain"), default="reference")
+    ap.add_argument("--assemble-only", action="store_true",
+                    help="write the fixture from the per-case results present in --parts, listing any missing case")
     args = ap.parse_args()
     os.makedirs(args.parts, exist_ok=True)
     params = sweep()
@@ -160,13 +162,18 @@ def main():
         pinned = []
     todo = sorted(set(sample) | set(pinned), key=lambda i: -(params[i][0] ** 3))
     jobs = [(i, params[i][0], params[i][1], i in pinned, args.parts, args.variant) for i in todo]
-    import multiprocessing as mp
-    with mp.get_context("spawn").Pool(args.workers) as pool:
-        for k, idx in enumerate(pool.imap_unordered(run_case, jobs)):
-            print(f"[{k + 1}/{len(jobs)}] case {idx} done", flush=True)
-    cases, fields = [], {}
+    if not args.assemble_only:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(args.workers) as pool:
+            for k, idx in enumerate(pool.imap_unordered(run_case, jobs)):
+                print(f"[{k + 1}/{len(jobs)}] case {idx} done", flush=True)
+    cases, fields, missing = [], {}, []
     for i in sorted(set(sample) | set(pinned)):
-        z = np.load(os.path.join(args.parts, f"case{i:03d}.npz"))
+        path = os.path.join(args.parts, f"case{i:03d}.npz")
+        if not os.path.exists(path):
+            missing.append(i)
+            continue
+        z = np.load(path)
         meta = json.loads(str(z["meta"]))
         meta["sample"], meta["pinned"] = i in sample, i in pinned
         cases.append(meta)
@@ -182,7 +189,7 @@ def main():
                           "machine, seconds_first3 of its first three iterations, seconds_to[k] up to first[k]; "
                           "diverged_at: the iteration whose residual was NaN. Written by make_sweep_oracle.py.",
            "sample": sample, "pinned": pinned, "grid_n": list(GRID_N), "grid_re": list(GRID_RE),
-           "cases": cases}
+           "missing": missing, "cases": cases}
     if args.variant == "plain":
         out["description"] = ("The oracle with the plain FP64 GPU form's settings (multicolour Gauss-Seidel as the "
                               "AMG smoother for p, DILU for U) on the 64-case sample of the 512-case 2D cavity sweep, "
