@@ -322,7 +322,9 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                launches=s1["graph_launches"] - s0["graph_launches"],
                graph_ticks=s1["graph_ticks"] - s0["graph_ticks"], ticks=s1["steps"] - s0["steps"],
                captures=s1["captures"] - s0["captures"], slot_drops=s1["slot_drops"] - s0["slot_drops"],
-               host_ms={k: round(s1[k] - s0[k], 1) for k in ("host_rebuild_ms", "host_capture_ms", "host_drop_ms")},
+               host_ms={k: round(s1[k] - s0[k], 1) for k in ("host_rebuild_ms", "host_capture_ms", "host_drop_ms",
+                                                            "build_wall_ms", "build_agg_ms", "build_color_ms",
+                                                            "build_ell_ms", "build_alloc_ms", "host_admit_ms")},
                peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
                tickets=tickets, tail=tail_profile(tick_log, len(specs)), admit_s=admit_s,
                cta_rows=s1["cta_rows"], tunes=s1["tunes"],
@@ -363,7 +365,8 @@ TICK_UNITS = (
     (2, "k_fcg_q (FP64 q = A p with (p, q) and (p, r), one per V-cycle)", lambda us, pc: pc, "hbm"),
     (6, "k_coarse_vcycle_pk (the levels below the grid levels, one CTA per large case or 4 small ones)",
      lambda us, pc: pc, "latency"),
-    (3, "k_uface + k_assemble_u + k_du_boundary (momentum assembly, 3 components)", lambda us, pc: 3, "hbm"),
+    (3, "k_uface_int + k_uface_bnd + k_assemble_u + k_du_boundary (momentum assembly, 3 components)",
+     lambda us, pc: 1, "hbm"),
     (4, "k_rhiechow + k_assemble_p (Rhie-Chow face flux and p matrix, 2 correctors)", lambda us, pc: 2, "hbm"),
     (5, "k_bc_update + k_grad_cells + k_grad_bfix + k_minmax_U (field update: gradients of U and p)",
      lambda us, pc: 1, "hbm"),

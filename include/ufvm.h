@@ -252,8 +252,11 @@ int ufvm_service_release(ufvm_service* s, int64_t ticket);
  * unreleased results, the memory budget, the admissions deferred for memory, the admissions
  * that failed to allocate and were re-queued, the departures of finished slots from the batch,
  * the footprint estimate's scale, the U-smoother and p-cycle loop bodies the replayed ticks
- * have run, and the host time (ms) spent rebuilding slot tables, capturing tick graphs and
- * freeing departed cases. Writes min(n, 28) values. */
+ * have run, the host time (ms) spent rebuilding slot tables, capturing tick graphs and
+ * freeing departed cases, the wall time (ms) of AMG hierarchy builds, the host time (ms) summed
+ * over the build threads in agglomeration, in colourings and FP32 arrays, in the ELL permutation
+ * and, of these, in device allocation calls, and the host time (ms) of admissions. Writes
+ * min(n, 34) values. */
 int ufvm_service_stats(ufvm_service* s, double* out, int n);
 /* Admits queued cases now, as far as the budgets allow, without waiting for the next step: their
  * meshes are uploaded and processed on the service stream, so a caller can have a batch resident

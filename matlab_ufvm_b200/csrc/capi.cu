@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" boundary of libufvm.so (declared in include/ufvm.h) and the
 // steady SIMPLE driver (top/cfdRunCase.m:92-142).
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -11,6 +12,9 @@ namespace ufvm {
 static thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
 const char* get_error() { return g_err.c_str(); }
+double host_ms_now() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 Case::~Case() {
   if (amg) {

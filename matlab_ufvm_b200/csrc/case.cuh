@@ -120,7 +120,7 @@ struct FieldView {
   double *DU0, *DU1, *DU2, *mdot, *fC1, *fC2;
   const double *vU0, *vU1, *vU2, *vP;  // boundary values (per boundary face)
   double* tmp3;                        // [Fb][3] staging for outlet velocity rows
-  double* uft;                         // [7][F] per-face momentum terms of one component
+  double* uft;                         // [3][7][F] per-face momentum terms of each component
 };
 
 // Per-case descriptor read by the batched kernels. A stage kernel is launched over a

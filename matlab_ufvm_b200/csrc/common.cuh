@@ -52,43 +52,87 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
 // service takes differences of it around each case's allocations to learn the case's HBM
 // footprint.
 inline thread_local long long t_dev_bytes = 0;
+// Host time (ms) this thread has spent inside device allocation and free calls.
+inline thread_local double t_alloc_ms = 0.0;
+
+// Stream-ordered allocation. A thread inside an AllocStreamScope allocates from the device's
+// default memory pool on the scope's stream (cudaMallocAsync) and frees there (cudaFreeAsync):
+// neither call waits for the device, while cudaFree waits for the whole device and cudaMalloc
+// goes through the driver's allocator. The batched service builds hundreds of cases' meshes and
+// AMG hierarchies on several host threads at once (hundreds of allocations per case), so it
+// allocates this way; everything else uses cudaMalloc. An array remembers how it was allocated.
+// An allocation is ordered on the scope's stream: work on another stream that uses it first
+// waits for that stream (the service's builders synchronise their streams before the service
+// stream uses what they made).
+inline thread_local cudaStream_t t_alloc_stream = nullptr;
+struct AllocStreamScope {
+  cudaStream_t prev;
+  explicit AllocStreamScope(cudaStream_t s) : prev(t_alloc_stream) { t_alloc_stream = s; }
+  ~AllocStreamScope() { t_alloc_stream = prev; }
+  AllocStreamScope(const AllocStreamScope&) = delete;
+  AllocStreamScope& operator=(const AllocStreamScope&) = delete;
+};
+// The scope's stream, or null when this thread should use cudaMalloc (no scope, or the stream is
+// being captured into a graph, where an asynchronous allocation would become a graph node).
+inline cudaStream_t alloc_stream_now() {
+  if (!t_alloc_stream) return nullptr;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(t_alloc_stream, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return cs == cudaStreamCaptureStatusNone ? t_alloc_stream : nullptr;
+}
+double host_ms_now();
 
 // Device array owned by a case; freed by its owner.
 template <typename T>
 struct DArr {
   T* p = nullptr;
   size_t n = 0;
+  bool async = false;  // allocated by cudaMallocAsync (stream-ordered), else cudaMalloc
 };
+
+template <typename T>
+void dfree(DArr<T>& a) {
+  if (a.p) {
+    const double t0 = host_ms_now();
+    if (!a.async) {
+      cudaFree(a.p);
+    } else if (cudaStream_t s = alloc_stream_now()) {
+      cudaFreeAsync(a.p, s);
+    } else {
+      // outside a scope nothing orders the free after the array's last use: wait for it
+      cudaDeviceSynchronize();
+      cudaFree(a.p);
+    }
+    t_alloc_ms += host_ms_now() - t0;
+    t_dev_bytes -= (long long)(a.n * sizeof(T));
+  }
+  a.p = nullptr;
+  a.n = 0;
+  a.async = false;
+}
 
 template <typename T>
 int dalloc(DArr<T>& a, size_t n) {
   if (a.p && a.n >= n) return UFVM_OK;
-  if (a.p) {
-    cudaFree(a.p);
-    t_dev_bytes -= (long long)(a.n * sizeof(T));
-  }
-  a.p = nullptr;
-  a.n = 0;
+  dfree(a);
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void**)&a.p, n * sizeof(T));
+  const double t0 = host_ms_now();
+  cudaStream_t s = alloc_stream_now();
+  cudaError_t e = s ? cudaMallocAsync((void**)&a.p, n * sizeof(T), s) : cudaMalloc((void**)&a.p, n * sizeof(T));
+  t_alloc_ms += host_ms_now() - t0;
   if (e != cudaSuccess) {
     a.p = nullptr;
     cudaGetLastError();  // an out-of-memory report is not sticky: clear it for later checks
-    set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    set_error(std::string(s ? "cudaMallocAsync: " : "cudaMalloc: ") + cudaGetErrorString(e));
     return UFVM_E_OOM;
   }
   a.n = n;
+  a.async = s != nullptr;
   t_dev_bytes += (long long)(n * sizeof(T));
   return UFVM_OK;
-}
-template <typename T>
-void dfree(DArr<T>& a) {
-  if (a.p) {
-    cudaFree(a.p);
-    t_dev_bytes -= (long long)(a.n * sizeof(T));
-  }
-  a.p = nullptr;
-  a.n = 0;
 }
 
 // ---- block reductions (fixed shape => deterministic) ----

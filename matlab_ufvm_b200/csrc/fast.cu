@@ -18,6 +18,7 @@
 // A step without hierarchy builds is captured once and replayed as a CUDA graph whose solve
 // loops are conditional WHILE nodes ended on the device.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <thread>
@@ -1085,13 +1086,15 @@ BatchLaunch Service::batch() {
 }
 
 // The reference's agglomeration of the assembled p matrix, FP32 arrays and colourings.
-int Service::ensure_hierarchy(Case& c, cudaStream_t st) {
+int Service::ensure_hierarchy(Case& c, cudaStream_t st, double* ms) {
   const long long b0 = t_dev_bytes;
+  const double a0 = t_alloc_ms;
   cudaStream_t own = c.lin.stream;
   c.lin.stream = st;  // the case's scratch and solver work run on `st` for the build
-  const int rc = ensure_hierarchy_(c, st);
+  const int rc = ensure_hierarchy_(c, st, ms);
   c.lin.stream = own;
   c.dev_bytes += t_dev_bytes - b0;
+  ms[3] += t_alloc_ms - a0;
   return rc;
 }
 
@@ -1102,9 +1105,20 @@ int Service::ensure_hierarchy(Case& c, cudaStream_t st) {
 // of them. A build's result does not depend on which thread or stream ran it.
 int Service::build_hierarchies(std::vector<Case*>& need) {
   if (need.empty()) return UFVM_OK;
+  const double w0 = host_ms_now();
   const int nt = (int)std::min<size_t>(need.size(), kBuildThreads);
+  std::vector<std::array<double, 4>> ms(std::max(nt, 1), std::array<double, 4>{0.0, 0.0, 0.0, 0.0});
+  auto account = [&]() {
+    for (const auto& m : ms)
+      for (int k = 0; k < 4; ++k) build_ms[k] += m[k];
+    build_wall_ms += host_ms_now() - w0;
+  };
   if (nt <= 1) {
-    for (Case* c : need) UFVM_CHECK(ensure_hierarchy(*c, stream));
+    for (Case* c : need) {
+      const int r = ensure_hierarchy(*c, stream, ms[0].data());
+      if (r != UFVM_OK) return r;
+    }
+    account();
     return UFVM_OK;
   }
   int dev = 0;
@@ -1125,8 +1139,9 @@ int Service::build_hierarchies(std::vector<Case*>& need) {
       msg[w] = "a hierarchy build thread could not join the service's device or stream";
       return;
     }
+    AllocStreamScope scope(build_streams[w]);  // this thread's allocations are ordered on its stream
     for (size_t k = next++; k < need.size(); k = next++) {
-      const int r = ensure_hierarchy(*need[k], build_streams[w]);
+      const int r = ensure_hierarchy(*need[k], build_streams[w], ms[w].data());
       if (r != UFVM_OK) {
         rc[w] = r;
         msg[w] = get_error();
@@ -1147,12 +1162,16 @@ int Service::build_hierarchies(std::vector<Case*>& need) {
       set_error(msg[w]);
       return rc[w];
     }
+  account();
   return UFVM_OK;
 }
 
-int Service::ensure_hierarchy_(Case& c, cudaStream_t st) {
+int Service::ensure_hierarchy_(Case& c, cudaStream_t st, double* ms) {
   c.amg->smoother = UFVM_SMOOTHER_MCGS; c.amg->quirks = c.S.quirks;
+  double t0 = host_ms_now();
   UFVM_CHECK(c.amg->build(c.lev, c.S.p_max_coarse_levels, c.S.quirks, &c.n_levels));
+  double t1 = host_ms_now();
+  ms[0] += t1 - t0;
   for (int l = 0; l < c.n_levels; ++l) {
     Level& L = c.lev[l];
     UFVM_CHECK(dalloc(L.ac32, L.n));
@@ -1167,7 +1186,10 @@ int Service::ensure_hierarchy_(Case& c, cudaStream_t st) {
       UFVM_CHECK(dalloc(L.fq, L.n));
     }
   }
+  t0 = host_ms_now();
+  ms[1] += t0 - t1;
   if (c.n_levels > 1) UFVM_CHECK(build_ell(c, st));
+  ms[2] += host_ms_now() - t0;
   c.hierarchy_valid = true;
   return UFVM_OK;
 }
@@ -1471,7 +1493,8 @@ int Service::enqueue_tick(bool g, std::vector<std::pair<int, int>>& marks) {
   UFVM_CHECK(stage_update_fields(b));
   for (int comp = 0; comp < 3; ++comp) {
     UFVM_CHECK(mark(PH_ASM_U));
-    UFVM_CHECK(stage_assemble_u(b, comp));
+    if (comp == 0) UFVM_CHECK(stage_uface_interior(b));
+    UFVM_CHECK(stage_assemble_u(b, comp, true));
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_RMS, SCAL_U_RMS + comp);
     k_copy_scal<<<nblocks(ns), kBlock, 0, stream>>>(slotTab.p, ns, SCAL_MAX, SCAL_U_MAX + comp);
     UFVM_CHECK(mark(PH_SOLVE_U));
@@ -1722,9 +1745,11 @@ int Service::iterate(std::vector<double>& res, std::vector<int>& conv) {
 //   1: the same sweep in FP32 over the V-cycle's level 0 (k_mc32, colour-permuted ELL):
 //      2 x (16 B per row -- ac, bc, x written, x read once -- + 8 B per nonzero);
 //   2: the flexible-CG product q = A p with its two dot products (k_fcg_q): 36 B/row + 12 B/nz;
-//   3: the momentum assembly of one component (k_uface, k_assemble_u, k_du_boundary and the
-//      residual reduction): per cell 8 phi + 24 grad phi + 16 (ac, bc), per interior face
-//      8 index + 8 mdot + 8 gamma + 8 gDiff + 24 T + 8 gf + 16 (two off-diagonals) bytes;
+//   3: the momentum assembly of the three components as a tick runs it (k_uface_int over the
+//      interior faces for all three, then per component k_uface_bnd, k_assemble_u, k_du_boundary
+//      and the residual reduction): per component, per cell 8 phi + 24 grad phi + 16 (ac, bc),
+//      per interior face 8 index + 8 mdot + 8 gamma + 8 gDiff + 24 T + 8 gf + 16 (two
+//      off-diagonals) bytes;
 //   4: the pressure-correction assembly (k_rhiechow, k_assemble_p and the mass-imbalance
 //      reduction): per cell 8 p + 24 grad p + 24 U + 24 DU + 16 (ac, bc), per interior face
 //      8 index + 8 gf + 24 Sf + 24 eCF + 8 |CF| + 8 mdot old + 8 mdot new + 16 (C1, C2) +
@@ -1769,7 +1794,9 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
                                           reinterpret_cast<double2*>(fcg.p + (((size_t)nwc + 1) & ~(size_t)1) +
                                                                      (((size_t)ns + 1) & ~(size_t)1)));
     } else if (kernel == 3) {
-      UFVM_CHECK(stage_assemble_u(batch(), 0));
+      const BatchLaunch b = batch();
+      UFVM_CHECK(stage_uface_interior(b));
+      for (int comp = 0; comp < 3; ++comp) UFVM_CHECK(stage_assemble_u(b, comp, true));
     } else if (kernel == 4) {
       UFVM_CHECK(stage_assemble_p(batch()));
     } else if (kernel == 5) {
@@ -1829,7 +1856,7 @@ int Service::profile(int kernel, int reps, double* ms, double* bytes) {
   if (kernel == 0) *bytes = 2.0 * (32.0 * N + 12.0 * NNZ) - (32.0 * skipN + 12.0 * skipNNZ);
   else if (kernel == 1) *bytes = 2.0 * (16.0 * N + 8.0 * NNZ) - (16.0 * skipN + 8.0 * skipNNZ);
   else if (kernel == 2) *bytes = 36.0 * N + 12.0 * NNZ;
-  else if (kernel == 3) *bytes = 48.0 * N + 80.0 * Fi;
+  else if (kernel == 3) *bytes = 3.0 * (48.0 * N + 80.0 * Fi);
   else if (kernel == 4) *bytes = 96.0 * N + 120.0 * Fi;
   else if (kernel == 5) *bytes = (3 * 32.0 + 32.0) * R + 2 * (24.0 * F + 16.0 * Fi + 8.0 * N);
   else {

@@ -30,7 +30,7 @@ struct LevDesc {
 // Packed coarse V-cycle: CTAs of kBlockPack threads; a task gives one large case the whole
 // CTA or each of kPackGroups thread groups its own small case (slot -1: none).
 constexpr int kBlockPack = 1024;
-constexpr size_t kBuildThreads = 8;  // host threads that build new cases' AMG hierarchies
+constexpr size_t kBuildThreads = 16;  // host threads that build new cases' AMG hierarchies
 constexpr int kPackGroups = 4;
 struct PackTask {
   int big;
@@ -129,6 +129,9 @@ struct Service {
   // host time (ms) spent rebuilding the slot tables and capturing the tick graph, in total and
   // for the most recent change of the slot set
   double host_rebuild_ms = 0.0, host_capture_ms = 0.0, last_rebuild_ms = 0.0;
+  // hierarchy builds: wall ms, and host ms summed over the build threads in agglomeration,
+  // colourings and FP32 arrays, ELL permutation, and (part of those) device allocation calls
+  double build_wall_ms = 0.0, build_ms[4] = {0.0, 0.0, 0.0, 0.0};
   // kernel launches: kernels of the captured tick outside the loops and per loop body, and
   // the device counters of executed U / p loop bodies
   long long static_kernels = 0, ubody_kernels = 0, pbody_kernels = 0, launches_total = 0;
@@ -148,8 +151,10 @@ struct Service {
   int rebuild_tables();
   BatchLaunch batch();
   bool needs_hierarchy(const Case& c) const;
-  int ensure_hierarchy(Case& c, cudaStream_t st);  // adds the bytes it allocates to c.dev_bytes
-  int ensure_hierarchy_(Case& c, cudaStream_t st);
+  // adds the bytes it allocates to c.dev_bytes, and its host ms (agglomeration, colourings and
+  // FP32 arrays, ELL permutation, of these in allocation calls) to ms[0..3]
+  int ensure_hierarchy(Case& c, cudaStream_t st, double* ms);
+  int ensure_hierarchy_(Case& c, cudaStream_t st, double* ms);
   int build_hierarchies(std::vector<Case*>& need);
   int build_ell(Case& c, cudaStream_t st);
   std::vector<cudaStream_t> build_streams;  // streams of the hierarchy-build threads

@@ -79,13 +79,26 @@ struct ServiceImpl {
   // device time) stays below what dropping them costs on the host (the last rebuild of the slot
   // tables with its graph capture, plus freeing the departed cases)
   double waste_ms = 0.0, last_drop_ms = 0.0, host_drop_ms = 0.0;
+  double host_admit_ms = 0.0;  // host time in admissions
   // Cases that left the batch are not freed at once: freeing a case's device arrays
   // (cudaFree, which waits for the whole device) costs far more host time than the rest of a
   // departure. They wait here until admission finds too little memory, or the service ends.
   std::vector<Case*> graveyard;
   void bury() {
+    if (graveyard.empty()) return;
     for (Case* c : graveyard) delete c;
     graveyard.clear();
+    // the cases' arrays went back to the device's memory pool (stream-ordered frees on the
+    // service stream): once those frees have run, hand the pool's idle memory back to the device
+    if (cudaStreamSynchronize(svc.stream) == cudaSuccess) {
+      int dev = 0;
+      cudaMemPool_t pool = nullptr;
+      if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess ||
+          cudaMemPoolTrimTo(pool, 0) != cudaSuccess)
+        cudaGetLastError();
+    } else {
+      cudaGetLastError();
+    }
   }
   std::map<long long, int> inject_oom;  // fault injection: admissions of a ticket that fail as OOM
   double clock_ms = 0;  // accumulated device time of all steps
@@ -141,6 +154,29 @@ struct ServiceImpl {
 // its schedules and colour-major copies, and the agglomeration hierarchy with its FP32 and ELL
 // copies (about as much again as the level-0 matrix). The service scales it by the largest
 // ratio of measured to estimated bytes it has seen.
+// Device memory a new case can take: the driver's free bytes plus what the device's default
+// memory pool holds without an allocation in it (the service allocates from that pool, and the
+// pool keeps what departed cases gave back).
+static bool device_room(size_t* room) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  int dev = 0;
+  cudaMemPool_t pool = nullptr;
+  unsigned long long reserved = 0, used = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess) {
+    if (reserved > used) fr += (size_t)(reserved - used);
+  } else {
+    cudaGetLastError();
+  }
+  *room = fr;
+  return true;
+}
+
 static long long estimate_raw(long long Nc, long long F, long long Fi, long long nodes) {
   const long long Fb = F - Fi, R = Nc + Fb, nnz = 2 * Fi;
   const long long dbl = 19 * F + 4 * Nc + 23 * R + 10 * F + 8 * Nc + 2 * (nnz + 8 * Nc) + 4 * nnz;
@@ -235,11 +271,8 @@ static std::map<long long, Precreated> precreate(ServiceImpl& S) {
   std::vector<Pending*> pick;
   long long cells = S.resident_cells, bytes = S.slot_bytes() + S.snap_bytes, est_sum = 0;
   bool empty = S.svc.cases.empty();
-  size_t fr = 0, tot = 0;
-  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-    cudaGetLastError();
-    return out;
-  }
+  size_t fr = 0;
+  if (!device_room(&fr)) return out;
   for (Pending& p : S.queue) {
     const long long est = S.estimate(p.est_raw);
     if (!empty && (cells + p.cells > S.max_cells || bytes + est > S.max_bytes)) break;
@@ -265,6 +298,7 @@ static std::map<long long, Precreated> precreate(ServiceImpl& S) {
       cudaGetLastError();
       return;  // the cases this thread would have made are created by the loop instead
     }
+    AllocStreamScope scope(st);  // this thread's allocations are ordered on its stream
     for (size_t k = next++; k < pick.size(); k = next++) {
       const Pending& p = *pick[k];
       ufvm_mesh_desc d;
@@ -298,8 +332,17 @@ static std::map<long long, Precreated> precreate(ServiceImpl& S) {
   return out;
 }
 
+static int admit_(ServiceImpl& S);
+// Admission with its host time accounted (mesh uploads and processing of the admitted cases).
 static int admit(ServiceImpl& S) {
   if (!admission_due(S)) return UFVM_OK;
+  const double t0 = host_ms_now();
+  const int rc = admit_(S);
+  S.host_admit_ms += host_ms_now() - t0;
+  return rc;
+}
+
+static int admit_(ServiceImpl& S) {
   drop_frozen(S);  // departures are gathered into the admission's table rebuild
   const size_t before = S.svc.cases.size();
   std::map<long long, Precreated> pre = precreate(S);
@@ -316,8 +359,8 @@ static int admit(ServiceImpl& S) {
     if (!S.svc.cases.empty()) {
       if (S.resident_cells + p.cells > S.max_cells) break;
       if (S.slot_bytes() + S.snap_bytes + est > S.max_bytes) { ++S.n_deferred_mem; break; }
-      size_t fr = 0, tot = 0;
-      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (long long)fr < est + (est >> 3)) {
+      size_t fr = 0;
+      if (device_room(&fr) && (long long)fr < est + (est >> 3)) {
         if (!S.graveyard.empty()) {  // free the departed cases, then look again
           S.bury();
           continue;
@@ -519,8 +562,8 @@ int ufvm_service_create(const ufvm_settings* settings, int64_t max_resident_cell
     }
   }
   // default HBM budget: 90% of the device memory free when the service starts
-  size_t fr = 0, tot = 0;
-  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
+  size_t fr = 0;
+  if (!device_room(&fr)) fr = 0;
   S.max_bytes = (long long)(0.9 * (double)fr);
   *out = h;
   return UFVM_OK;
@@ -566,6 +609,7 @@ int ufvm_service_submit(ufvm_service* h, const ufvm_mesh_desc* m, double nu, con
 
 int ufvm_service_step(ufvm_service* h, int32_t* n_resident, int32_t* n_queued, int64_t* n_finished_total) {
   if (!h) return UFVM_E_INVALID;
+  AllocStreamScope alloc_scope(h->impl.svc.stream);  // the service allocates on its stream
   ServiceImpl& S = h->impl;
   Service& V = S.svc;
   {
@@ -695,6 +739,7 @@ int ufvm_service_get_field(ufvm_service* h, int64_t ticket, const char* name, do
 
 int ufvm_service_release(ufvm_service* h, int64_t ticket) {
   if (!h) return UFVM_E_INVALID;
+  AllocStreamScope alloc_scope(h->impl.svc.stream);  // the service allocates on its stream
   auto it = h->impl.rec.find(ticket);
   if (it == h->impl.rec.end()) return UFVM_OK;
   if (it->second.state == 1) { set_error("ticket is still resident"); return UFVM_E_INVALID; }
@@ -743,6 +788,9 @@ int ufvm_service_stats(ufvm_service* h, double* out, int n) {
   v.push_back(V.host_rebuild_ms);
   v.push_back(V.host_capture_ms);
   v.push_back(h->impl.host_drop_ms);
+  v.push_back(V.build_wall_ms);
+  for (int k = 0; k < 4; ++k) v.push_back(V.build_ms[k]);
+  v.push_back(h->impl.host_admit_ms);
   for (int i = 0; i < n; ++i) out[i] = i < (int)v.size() ? v[i] : 0.0;
   return UFVM_OK;
 }
@@ -750,6 +798,7 @@ int ufvm_service_stats(ufvm_service* h, double* out, int n) {
 int ufvm_service_profile(ufvm_service* h, int32_t kernel, int32_t reps, double* ms_per_unit,
                          double* bytes_per_unit) {
   if (!h || !ms_per_unit || !bytes_per_unit) return UFVM_E_INVALID;
+  AllocStreamScope alloc_scope(h->impl.svc.stream);  // the service allocates on its stream
   return h->impl.svc.profile(kernel, reps, ms_per_unit, bytes_per_unit);
 }
 
@@ -765,6 +814,7 @@ int ufvm_service_poll(ufvm_service* h, int64_t* tickets, int64_t capacity, int64
 
 int ufvm_service_admit(ufvm_service* h, int32_t* n_resident) {
   if (!h) return UFVM_E_INVALID;
+  AllocStreamScope alloc_scope(h->impl.svc.stream);  // the service allocates on its stream
   ServiceImpl& S = h->impl;
   S.steps_since_admit = 1 << 30;  // due now
   UFVM_CHECK(admit(S));
@@ -820,11 +870,20 @@ int ufvm_service_stream(ufvm_service* h, void** stream) {
 
 int ufvm_service_destroy(ufvm_service* h) {
   if (!h) return UFVM_OK;
+  {
+    AllocStreamScope alloc_scope(h->impl.svc.stream);
   // cases in slots (active or frozen) are owned by the Service; the rest by their records
   for (auto& kv : h->impl.rec)
     for (Case* c : h->impl.svc.cases)
       if (kv.second.c == c) kv.second.c = nullptr;
-  delete h;
+    delete h;
+  }
+  // give the memory the service's arrays held in the device's default pool back to the device
+  int dev = 0;
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess || cudaMemPoolTrimTo(pool, 0) != cudaSuccess)
+    cudaGetLastError();
   return UFVM_OK;
 }
 

@@ -219,7 +219,7 @@ int Case::init_fields(const int32_t* bcu, const int32_t* bcp, const double* vu, 
     UFVM_CUDA(cudaMemsetAsync(DU[c].p, 0, R * sizeof(double), stream));
   }
   UFVM_CHECK(dalloc(mdot, F));
-  UFVM_CHECK(dalloc(uft, 7 * (size_t)F));
+  UFVM_CHECK(dalloc(uft, 3 * 7 * (size_t)F));  // [comp][term][face]
   UFVM_CHECK(dalloc(fC1, F));
   UFVM_CHECK(dalloc(fC2, F));
   UFVM_CUDA(cudaMemsetAsync(fC1.p, 0, F * sizeof(double), stream));

@@ -262,7 +262,7 @@ __device__ __forceinline__ void face_grad_corr(const MeshView& m, int fc, int o,
 // convection coefficients and flux (cfdAssembleConvectionTerm.m:103-232), the diffusion
 // coefficients and flux (cfdAssembleDiffusionTerm.m:94-690; Q3, Q4, Q14, Q15) and the explicit
 // stress flux (cfdAssembleExplicitStressTerm.m:13-49, Q2), computed once per face (each
-// interior face serves two cells) into uft[k][F]:
+// interior face serves two cells) into uft[comp][k][F]:
 //   k = 0, 1, 2: convection C1, C2, T;  3, 4, 5: diffusion C1, C2, T;  6: stress T.
 // The cell kernel below adds them exactly as the reference's scatter does.
 enum { UF_C1 = 0, UF_C2 = 1, UF_T = 2, UF_D1 = 3, UF_D2 = 4, UF_TD = 5, UF_TS = 6, UF_N = 7 };
@@ -272,17 +272,91 @@ enum { UF_C1 = 0, UF_C2 = 1, UF_T = 2, UF_D1 = 3, UF_D2 = 4, UF_TD = 5, UF_TS = 
 __device__ __forceinline__ double conv_c1(double psi) { return 1.0 * dmax(psi, 0.0); }
 __device__ __forceinline__ double conv_c2(double psi) { return -1.0 * dmax(-psi, 0.0); }
 
-__global__ void __launch_bounds__(kBlock, 4) k_uface(const SlotDesc* __restrict__ slots,
-                                                     const int2* __restrict__ work, int comp) {
+// Interior faces: the face terms of components c0..c1, stored at uft + comp * UF_N * F. The
+// face's geometry, mass flux and cells are read once for all the components it forms. An
+// interior face's terms depend only on the cells' values of the component, the gradients of
+// the iteration and the mass flux, none of which the solve and correction of another component
+// change (they write that component's cells and boundary values), so the service forms all
+// three components' interior terms before the first component's solve.
+__global__ void __launch_bounds__(kBlock, 3) k_uface_int(const SlotDesc* __restrict__ slots,
+                                                         const int2* __restrict__ work, int c0, int c1) {
   SLOT_BEGIN(work);
   const int fc = idx;
-  if (fc >= m.F) return;
+  if (fc >= m.Fi) return;
+  const FieldView& f = S.f;
+  const int quirks = S.quirks;
+  const bool q4 = (quirks & UFVM_Q4_GRAD_WEIGHTS_SWAPPED) != 0;
+  const bool q2 = (quirks & UFVM_Q2_STRESS_NOT_TRANSPOSED) != 0;
+  const double nu = S.nu;
+  const size_t F = (size_t)m.F;
+  const int o = m.owner[fc], n = m.neigh[fc];
+  const double psi = f.mdot[fc];
+  const double w = m.gf[fc];
+  const double gD = m.gDiff[fc];
+  const double d0 = m.CNx[fc], d1 = m.CNy[fc], d2 = m.CNz[fc];
+  const double t0 = m.Tx[fc], t1 = m.Ty[fc], t2 = m.Tz[fc];
+  const double sx = m.Sx[fc], sy = m.Sy[fc], sz = m.Sz[fc];
+  const double gam = w * nu + (1 - w) * nu;
+  const double dmag = sqrt(dot3(d0, d1, d2, d0, d1, d2));
+  const double e0 = d0 / dmag, e1 = d1 / dmag, e2 = d2 / dmag;
+#pragma unroll 1
+  for (int comp = c0; comp <= c1; ++comp) {
+    const double* ph = Uc(f, comp);
+    const double* g0 = f.gU[comp * 3];
+    const double* g1 = f.gU[comp * 3 + 1];
+    const double* g2 = f.gU[comp * 3 + 2];
+    const double* s0 = q2 ? f.gU[comp * 3 + 0] : f.gU[0 * 3 + comp];
+    const double* s1 = q2 ? f.gU[comp * 3 + 1] : f.gU[1 * 3 + comp];
+    const double* s2 = q2 ? f.gU[comp * 3 + 2] : f.gU[2 * 3 + comp];
+    const double pho = ph[o], phn = ph[n];
+    double Tc, D1, D2, TD, TS;
+    {  // (1) convection, sign +1; C1, C2 of an interior face are recomputed from mdot by the cell kernel
+      const double C1 = conv_c1(psi);
+      const double C2 = conv_c2(psi);
+      Tc = (C1 * pho + C2 * phn) + 0.0;
+    }
+    {  // (2) diffusion, sign -1, with the Average:Corrected face gradient
+      // (interpolate/cfdInterpolateGradientsFromElementsToInteriorFaces.m:23-70; Q4 weights)
+      double a0, a1, a2;
+      if (q4) {
+        a0 = (1 - w) * g0[n] + w * g0[o]; a1 = (1 - w) * g1[n] + w * g1[o]; a2 = (1 - w) * g2[n] + w * g2[o];
+      } else {
+        a0 = w * g0[n] + (1 - w) * g0[o]; a1 = w * g1[n] + (1 - w) * g1[o]; a2 = w * g2[n] + (1 - w) * g2[o];
+      }
+      const double lgm = (phn - pho) / dmag;
+      const double agm = dot3(a0, a1, a2, e0, e1, e2);
+      const double gf0 = (a0 - agm * e0) + lgm * e0;
+      const double gf1 = (a1 - agm * e1) + lgm * e1;
+      const double gf2 = (a2 - agm * e2) + lgm * e2;
+      D1 = (1.0 * gam) * gD;
+      D2 = (-1.0 * gam) * gD;
+      const double V = (-1.0 * gam) * dot3(gf0, gf1, gf2, t0, t1, t2);
+      TD = (D1 * pho + D2 * phn) + V;
+    }
+    {  // (3) explicit stress, sign -1
+      const double x0 = w * s0[n] + (1 - w) * s0[o], x1 = w * s1[n] + (1 - w) * s1[o];
+      const double x2 = w * s2[n] + (1 - w) * s2[o];
+      TS = (-1.0 * gam) * ((x0 * sx + x1 * sy) + x2 * sz);
+    }
+    double* u = f.uft + (size_t)comp * UF_N * F;
+    u[UF_T * F + fc] = Tc;
+    u[UF_D1 * F + fc] = D1; u[UF_D2 * F + fc] = D2; u[UF_TD * F + fc] = TD;
+    u[UF_TS * F + fc] = TS;
+  }
+}
+
+// Boundary faces: the face terms of one component (they read the other components' boundary and
+// owner values, which the earlier components' corrections have changed).
+__global__ void __launch_bounds__(kBlock, 4) k_uface_bnd(const SlotDesc* __restrict__ slots,
+                                                         const int2* __restrict__ work, int comp) {
+  SLOT_BEGIN(work);
+  if (idx >= m.Fb) return;
+  const int fc = m.Fi + idx;
   const FieldView& f = S.f;
   const int quirks = S.quirks;
   const double* ph = Uc(f, comp);
   const double nu = S.nu;
   const double psi = f.mdot[fc];
-  const bool q4 = (quirks & UFVM_Q4_GRAD_WEIGHTS_SWAPPED) != 0;
   const double* g0 = f.gU[comp * 3];
   const double* g1 = f.gU[comp * 3 + 1];
   const double* g2 = f.gU[comp * 3 + 2];
@@ -290,45 +364,18 @@ __global__ void __launch_bounds__(kBlock, 4) k_uface(const SlotDesc* __restrict_
   const double* s0 = q2 ? f.gU[comp * 3 + 0] : f.gU[0 * 3 + comp];
   const double* s1 = q2 ? f.gU[comp * 3 + 1] : f.gU[1 * 3 + comp];
   const double* s2 = q2 ? f.gU[comp * 3 + 2] : f.gU[2 * 3 + comp];
-  double* u = f.uft;
   const size_t F = (size_t)m.F;
-  if (fc < m.Fi) {
-    const int o = m.owner[fc], n = m.neigh[fc];
-    {  // (1) convection, sign +1
-      const double C1 = conv_c1(psi);
-      const double C2 = conv_c2(psi);
-      const double T = (C1 * ph[o] + C2 * ph[n]) + 0.0;
-      u[UF_T * F + fc] = T;  // C1, C2 of an interior face: recomputed from mdot by the cell kernel
-    }
-    const double w = m.gf[fc];
-    const double gam = w * nu + (1 - w) * nu;
-    {  // (2) diffusion, sign -1
-      double gf0, gf1, gf2;
-      face_grad_corr(m, fc, o, n, g0, g1, g2, ph, q4, gf0, gf1, gf2);
-      const double C1 = (1.0 * gam) * m.gDiff[fc];
-      const double C2 = (-1.0 * gam) * m.gDiff[fc];
-      const double V = (-1.0 * gam) * dot3(gf0, gf1, gf2, m.Tx[fc], m.Ty[fc], m.Tz[fc]);
-      const double T = (C1 * ph[o] + C2 * ph[n]) + V;
-      u[UF_D1 * F + fc] = C1; u[UF_D2 * F + fc] = C2; u[UF_TD * F + fc] = T;
-    }
-    {  // (3) explicit stress, sign -1
-      const double x0 = w * s0[n] + (1 - w) * s0[o], x1 = w * s1[n] + (1 - w) * s1[o];
-      const double x2 = w * s2[n] + (1 - w) * s2[o];
-      u[UF_TS * F + fc] = (-1.0 * gam) * ((x0 * m.Sx[fc] + x1 * m.Sy[fc]) + x2 * m.Sz[fc]);
-    }
-    return;
-  }
+  double* u = f.uft + (size_t)comp * UF_N * F;
   const int e = m.owner[fc];
   const int kb = fc - m.Fi, b = m.Nc + kb, p = m.bPatch[kb];
   const int ty = m.ptype[p], tu = m.bcU[p];
+  double Cc = 0.0, Tc = 0.0;  // stored with the other terms at the end, as above
   {  // (1) convection
-    double C1 = 0.0, T = 0.0;
     if (ty == UFVM_PATCH_INLET || ty == UFVM_PATCH_OUTLET) {
-      C1 = 1.0 * dmax(psi, 0.0);
+      Cc = 1.0 * dmax(psi, 0.0);
       const double C2 = -1.0 * dmax(-psi, 0.0);
-      T = (C1 * ph[e] + C2 * ph[b]) + 0.0;
+      Tc = (Cc * ph[e] + C2 * ph[b]) + 0.0;
     }
-    u[UF_C1 * F + fc] = C1; u[UF_T * F + fc] = T;
   }
   const double gam = nu;
   {  // (2) diffusion
@@ -368,10 +415,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_uface(const SlotDesc* __restrict_
       const double V = (((((-1.0 * 2) * gam) * A) * dv) * nc) / dd;
       T = (C1 * ph[e] + 0.0 * ph[b]) + V;
     }
+    // (3) explicit stress
+    const double TS = (-1.0 * gam) * ((s0[b] * m.Sx[fc] + s1[b] * m.Sy[fc]) + s2[b] * m.Sz[fc]);
+    u[UF_C1 * F + fc] = Cc; u[UF_T * F + fc] = Tc;
     u[UF_D1 * F + fc] = C1; u[UF_TD * F + fc] = T;
+    u[UF_TS * F + fc] = TS;
   }
-  // (3) explicit stress
-  u[UF_TS * F + fc] = (-1.0 * gam) * ((s0[b] * m.Sx[fc] + s1[b] * m.Sy[fc]) + s2[b] * m.Sz[fc]);
 }
 
 constexpr int kCellFaces = 8;  // cells with at most this many faces take the register path
@@ -391,8 +440,8 @@ __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restric
     const int s = m.cfStart[e], ne = m.cfStart[e + 1];
     const int r0 = m.rowptr[e];
     double* anb = S.anb;
-    const double* u = f.uft;
     const size_t F = (size_t)m.F;
+    const double* u = f.uft + (size_t)comp * UF_N * F;
     double acv = 0.0, bcv = 0.0, eff = 0.0;
     const int nf = ne - s;
     if (nf <= kCellFaces) {
@@ -822,8 +871,15 @@ int stage_update_fields(const BatchLaunch& b) {
   return gradient<G_P>(b);
 }
 
-int stage_assemble_u(const BatchLaunch& b, int comp) {
-  k_uface<<<b.nwf, kBlock, 0, b.st>>>(b.slots, b.wf, comp);
+int stage_uface_interior(const BatchLaunch& b) {
+  k_uface_int<<<b.nwf, kBlock, 0, b.st>>>(b.slots, b.wf, 0, 2);
+  UFVM_LAUNCH_CHECK();
+  return UFVM_OK;
+}
+
+int stage_assemble_u(const BatchLaunch& b, int comp, bool interior_ready) {
+  if (!interior_ready) k_uface_int<<<b.nwf, kBlock, 0, b.st>>>(b.slots, b.wf, comp, comp);
+  k_uface_bnd<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, comp);
   k_assemble_u<<<b.nwc, kBlock, 0, b.st>>>(b.slots, b.wc, comp, b.part);
   k_du_boundary<<<b.nwb, kBlock, 0, b.st>>>(b.slots, b.wb, comp);
   k_slot_final<0><<<b.nslots, 1024, 0, b.st>>>(b.slots, b.cstart, b.cend, b.part);

@@ -481,8 +481,8 @@ class Service:
     PHASES = ("update", "assemble_u", "solve_u", "correct_u", "assemble_p", "hierarchy", "solve_p", "correct_p")
 
     def stats(self) -> Dict:
-        out = np.zeros(28)
-        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 28))
+        out = np.zeros(34)
+        _check(_service_lib().ufvm_service_stats(self.h, _dp(out), 34))
         d = {f"{k}_ms": float(out[i]) for i, k in enumerate(self.PHASES)}
         d.update(u_sweeps=int(out[8]), p_cycles=int(out[9]), steps=int(out[10]), clock_ms=float(out[11]),
                  graph_ticks=int(out[12]), captures=int(out[13]), graph_launches=int(out[14]),
@@ -490,7 +490,9 @@ class Service:
                  memory_budget=int(out[18]), deferred_for_memory=int(out[19]), oom_requeues=int(out[20]),
                  slot_drops=int(out[21]), footprint_scale=float(out[22]), u_loop_bodies=int(out[23]),
                  p_loop_bodies=int(out[24]), host_rebuild_ms=float(out[25]), host_capture_ms=float(out[26]),
-                 host_drop_ms=float(out[27]))
+                 host_drop_ms=float(out[27]), build_wall_ms=float(out[28]), build_agg_ms=float(out[29]),
+                 build_color_ms=float(out[30]), build_ell_ms=float(out[31]), build_alloc_ms=float(out[32]),
+                 host_admit_ms=float(out[33]))
         return d
 
     def admit(self) -> int:

@@ -436,8 +436,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     check(ufvm_service_set_schedule(service_of(prhs[1]), (int32_t)mxGetScalar(prhs[2]), (int32_t)mxGetScalar(prhs[3])));
   } else if (!strcmp(cmd, "service_stats")) {
     need_args(nrhs, 2, cmd);
-    plhs[0] = mxCreateDoubleMatrix(1, 28, mxREAL);
-    check(ufvm_service_stats(service_of(prhs[1]), mxGetDoubles(plhs[0]), 28));
+    plhs[0] = mxCreateDoubleMatrix(1, 34, mxREAL);
+    check(ufvm_service_stats(service_of(prhs[1]), mxGetDoubles(plhs[0]), 34));
   } else if (!strcmp(cmd, "service_destroy")) {
     ufvm_service* v;
     need_args(nrhs, 2, cmd);

@@ -11,9 +11,9 @@ compute/cfdComputeNormalizedResidual.m:27-88) first passes at each tolerance.
 
 The pinned cases run in the service (FP64 multicolour Gauss-Seidel for U, FP32 agglomeration
 AMG preconditioning FP64 flexible CG for p) to the tightest residualControl the oracle itself
-reached on the case (1e-11 on all but one, which stagnates at 1.3e-11 and gets 1e-10), and the
-fields are also read at the tick where the residuals first pass 1e-6 -- the iterate at which the
-bench's runs stop. Field error is the relative L2 distance of U (all three components over the
+reached on the case (1e-11 on all but two: n=27 Re=985 stagnates at 1.3e-11 and n=253 Re=121 at
+2.5e-11, so both get 1e-10), and the fields are also read at the tick where the residuals first
+pass 1e-6 -- the iterate at which the bench's runs stop. Field error is the relative L2 distance of U (all three components over the
 cells) and of p - p[cell 0] from the oracle's fixed point (its last iterate, stored in float32:
 about 6e-8 of rounding).
 
@@ -24,7 +24,10 @@ residual near 1e-11 for 1e-6). Checked, per case:
   1e-6 stop (at most SAME_SIZE times it);
 * for n <= 128, the service's 1e-6 fields against the oracle's 1e-6 fields (the same stopping
   rule on both sides) differ by less than the sum of the two stops' errors;
-* at the tight stop, the service's field error is <= 1e-6.
+* at the tight stop, the service's field error is <= 1e-6 beyond the
+  oracle's own error at that stop: zero where the oracle's fixed point is its 1e-11 iterate;
+  2.0e-6 (U) and 1.0e-6 (p) for n=253 Re=121, whose residual stagnates before its fields reach
+  1e-6 of the fixed point (the oracle's fields at 1e-10 are that far from its last iterate).
 """
 import json
 import os
@@ -103,6 +106,7 @@ def test_service_at_operating_point_against_oracle(ufvm_mod):
     report = []
     for c, r in zip(cases, res):
         i = c["index"]
+        tk = str(max(int(k) for k in c["first"]))
         Uf = z[f"U_fix_{i}"].astype(np.float64)
         pf = z[f"p_fix_{i}"].astype(np.float64)
         row = {"index": i, "n": c["n"], "re": round(c["re"], 1),
@@ -110,7 +114,8 @@ def test_service_at_operating_point_against_oracle(ufvm_mod):
                "service_err_u_1e-6": rel(r["U6"], Uf), "service_err_p_1e-6": _perr(r["p6"], pf),
                "oracle_err_u_1e-6": c["err_u"]["6"], "oracle_err_p_1e-6": c["err_p"]["6"],
                "tight_tol": tight_tol(c), "service_it_tight": r["it"], "service_err_u_tight": rel(r["U"], Uf),
-               "service_err_p_tight": _perr(r["p"], pf)}
+               "service_err_p_tight": _perr(r["p"], pf), "oracle_it_tight": c["first"][tk],
+               "oracle_err_u_tight": c["err_u"][tk], "oracle_err_p_tight": c["err_p"][tk]}
         if f"U_6_{i}" in z.files:
             row["same_rule_u"] = rel(r["U6"], z[f"U_6_{i}"].astype(np.float64))
             row["same_rule_p"] = _perr(r["p6"], z[f"p_6_{i}"].astype(np.float64))
@@ -121,7 +126,8 @@ def test_service_at_operating_point_against_oracle(ufvm_mod):
             json.dump({"cases": report}, f, indent=1)
     for row in report:
         what = f"n={row['n']} Re={row['re']}"
-        assert row["service_err_u_tight"] <= FIELD_TOL and row["service_err_p_tight"] <= FIELD_TOL, (what, row)
+        assert row["service_err_u_tight"] <= FIELD_TOL + row["oracle_err_u_tight"], (what, row)
+        assert row["service_err_p_tight"] <= FIELD_TOL + row["oracle_err_p_tight"], (what, row)
         assert row["service_err_u_1e-6"] <= SAME_SIZE * row["oracle_err_u_1e-6"] + FIELD_TOL, (what, row)
         assert row["service_err_p_1e-6"] <= SAME_SIZE * row["oracle_err_p_1e-6"] + FIELD_TOL, (what, row)
         if "same_rule_u" in row:
