@@ -257,8 +257,9 @@ def warm_up(args):
     return svc
 
 
-def run_batch(args, specs, ws, e2e: bool, rank: int):
-    """The timed batch: every case of `specs` to convergence in K steps of --ticks ticks."""
+def run_batch(args, specs, ws, e2e: bool, rank: int, keep=()):
+    """The timed batch: every case of `specs` to convergence in K steps of --ticks ticks. In the
+    e2e pass, the read-back U and p of the cases whose positions are in `keep` are returned too."""
     import torch
     svc = new_service(args)
     stream = torch.cuda.ExternalStream(svc.stream())
@@ -285,6 +286,8 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
         for s in specs:
             tickets.append(svc.submit(s, MAX_ITER))
             h2d += mesh_bytes(s)
+    keep_t = {tickets[i]: i for i in keep if i < len(tickets)}
+    kept = {}
     finished = {}
     remaining = len(specs)
     tick_log = []  # (active cases before the tick, device ms of the tick)
@@ -305,6 +308,8 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                     if st["state"] == "converged":
                         u, p = svc.field(t, "U"), svc.field(t, "p")
                         d2h += u.nbytes + p.nbytes
+                        if t in keep_t:
+                            kept[keep_t[t]] = (u, p)
                     svc.release(t)
                 finished[t] = st
                 remaining -= 1
@@ -327,7 +332,7 @@ def run_batch(args, specs, ws, e2e: bool, rank: int):
                                                             "build_ell_ms", "build_alloc_ms", "host_admit_ms")},
                peak_bytes=s1["resident_bytes"], h2d=h2d, d2h=d2h, clocks=clocks,
                tickets=tickets, tail=tail_profile(tick_log, len(specs)), admit_s=admit_s,
-               cta_rows=s1["cta_rows"], tunes=s1["tunes"],
+               cta_rows=s1["cta_rows"], tunes=s1["tunes"], kept=kept,
                first_tick_ms=tick_log[0][1] if tick_log else None)
     return svc, out
 
@@ -778,6 +783,61 @@ def plain_named_configs(channel=None):
     return out
 
 
+ORACLE_FIELDS = os.path.join(ROOT, "tests", "golden", "sweep_oracle_fields.npz")
+
+
+def oracle_pinned(rank: int):
+    """The pinned cases of the oracle fixture (cases of the seed-2024 batch run by the oracle to
+    their fixed point), for the rank whose batch that is."""
+    if rank != 0 or not os.path.exists(ORACLE_FIELDS):
+        return []
+    return [c for c in oracle_fixture()["cases"] if c["pinned"] and "diverged_at" not in c]
+
+
+def error_vs_oracle(pinned, specs, kept):
+    """Relative L2 distance of the bench's converged U and of p - p[cell 0] (read back in the e2e
+    pass, at the bench's residualControl stop of 1e-6) from the oracle's fixed point of the same
+    case, next to the oracle's own distance at its 1e-6 stop; and, where the fixture holds the
+    oracle's 1e-6 fields, the distance between the two 1e-6 stops."""
+    import numpy as np
+    z = np.load(ORACLE_FIELDS)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    rows = []
+    for c in pinned:
+        i = c["index"]
+        if i not in kept:
+            continue
+        nc = specs[i].mesh.n_cells
+        U = kept[i][0].reshape(3, -1)[:, :nc]
+        p = kept[i][1][:nc]
+        Uf, pf = z[f"U_fix_{i}"].astype(np.float64), z[f"p_fix_{i}"].astype(np.float64)
+        row = {"index": i, "n": c["n"], "u": rel(U, Uf), "p": rel(p - p[0], pf - pf[0]),
+               "u_oracle_own": c["err_u"]["6"], "p_oracle_own": c["err_p"]["6"]}
+        if f"U_6_{i}" in z.files:
+            U6, p6 = z[f"U_6_{i}"].astype(np.float64), z[f"p_6_{i}"].astype(np.float64)
+            row["u_same_rule"] = rel(U, U6)
+            row["p_same_rule"] = rel(p - p[0], p6 - p6[0])
+        rows.append(row)
+    if not rows:
+        return None
+    q = lambda k: {"p50": pct([r[k] for r in rows], 50), "max": max(r[k] for r in rows)}
+    same = [r for r in rows if "u_same_rule" in r]
+    out = {"cases": len(rows), "u_rel_l2": q("u"), "p_rel_l2": q("p"),
+           "u_over_oracle_own": {"min": min(r["u"] / r["u_oracle_own"] for r in rows),
+                                 "max": max(r["u"] / r["u_oracle_own"] for r in rows)},
+           "p_over_oracle_own": {"min": min(r["p"] / r["p_oracle_own"] for r in rows),
+                                 "max": max(r["p"] / r["p_oracle_own"] for r in rows)},
+           "what": "relative L2 of U and of p - p[cell 0] at the bench's 1e-6 stop against the oracle's "
+                   "fixed point of the same case (the pinned cases of tests/golden/sweep_oracle.json, "
+                   "one per (n, Re) grid point); u/p_over_oracle_own: that error over the oracle's own "
+                   "distance from its fixed point at its 1e-6 stop"}
+    if same:
+        out["same_rule"] = {"cases": len(same), "u_max": max(r["u_same_rule"] for r in same),
+                            "p_max": max(r["p_same_rule"] for r in same),
+                            "what": "the bench's 1e-6 fields against the oracle's 1e-6 fields (n <= 128)"}
+    return out
+
+
 def main_ours(args):
     import torch
     rank, ws, local = dist_setup(args) if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 \
@@ -804,9 +864,13 @@ def main_ours(args):
     ttc = gather_list(res["ttc"], ws)
     iters = gather_list(res["iters"], ws)
     e2e = None
+    pinned = oracle_pinned(rank) if os.path.exists(ORACLE_FIXTURE) else []
+    errors = None
     if not args.no_e2e:
-        svc2, r2 = run_batch(args, specs, ws, e2e=True, rank=rank)
+        svc2, r2 = run_batch(args, specs, ws, e2e=True, rank=rank, keep=[c["index"] for c in pinned])
         svc2.close()
+        if pinned:
+            errors = error_vs_oracle(pinned, specs, r2["kept"])
         tot2 = reduce_sum(r2["converged"], ws)
         wall2 = reduce_max(r2["wall"], ws)
         e2e = {"value": tot2 / wall2 if wall2 > 0 else 0.0, "unit": "cases/s",
@@ -853,6 +917,7 @@ def main_ours(args):
             "admission_s_before_timing": round(res["admit_s"], 3) if res["admit_s"] is not None else None,
             "first_tick_ms": res["first_tick_ms"], "cta_rows": res["cta_rows"],
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res["clocks"],
+            "error_vs_oracle": errors,
         }
         if cpu:
             line["cpu_baseline"] = {

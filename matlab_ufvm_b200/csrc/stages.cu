@@ -448,14 +448,17 @@ __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restric
       // The cell's face list, its side of each face (owner, neighbour, boundary) and its row of
       // off-diagonals are read or built once and kept in registers; the three passes below add
       // the same terms in the same order as the general loops after them.
-      int fcs[kCellFaces], side[kCellFaces];
+      // side of face j in bits 2j..2j+1: 1 owner, 2 neighbour, 0 boundary
+      int fcs[kCellFaces];
+      unsigned sides = 0;
       double an[kCellFaces];
 #pragma unroll
       for (int j = 0; j < kCellFaces; ++j)
         if (j < nf) {
           fcs[j] = m.cfFace[s + j];
-          side[j] = fcs[j] < m.Fi ? (m.owner[fcs[j]] == e ? 1 : -1) : 0;
+          sides |= (fcs[j] < m.Fi ? (m.owner[fcs[j]] == e ? 1u : 2u) : 0u) << (2 * j);
         }
+#define SIDE(j) ((sides >> (2 * (j))) & 3u)
       // (1) convection, sign +1
 #pragma unroll
       for (int j = 0; j < kCellFaces; ++j)
@@ -463,10 +466,10 @@ __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restric
           const int fc = fcs[j];
           const double psi = f.mdot[fc];
           const double T = u[UF_T * F + fc];
-          if (side[j] > 0) {
+          if (SIDE(j) == 1u) {
             const double C2 = conv_c2(psi);
             acv = acv + conv_c1(psi); an[j] = 0.0 + C2; bcv = bcv - T; eff = eff + psi;
-          } else if (side[j] < 0) {
+          } else if (SIDE(j) == 2u) {
             const double C2 = conv_c2(psi);
             acv = acv - C2; an[j] = 0.0 - conv_c1(psi); bcv = bcv + T; eff = eff - psi;
           } else {
@@ -486,10 +489,10 @@ __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restric
         if (j < nf) {
           const int fc = fcs[j];
           const double C1 = u[UF_D1 * F + fc], T = u[UF_TD * F + fc];
-          if (side[j] > 0) {
+          if (SIDE(j) == 1u) {
             const double C2 = u[UF_D2 * F + fc];
             acv = acv + C1; an[j] = an[j] + C2; bcv = bcv - T;
-          } else if (side[j] < 0) {
+          } else if (SIDE(j) == 2u) {
             const double C2 = u[UF_D2 * F + fc];
             acv = acv - C2; an[j] = an[j] - C1; bcv = bcv + T;
           } else {
@@ -501,13 +504,14 @@ __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restric
       for (int j = 0; j < kCellFaces; ++j)
         if (j < nf) {
           const double T = u[UF_TS * F + fcs[j]];
-          if (side[j] > 0) { acv = acv + 0.0; an[j] = an[j] + 0.0; bcv = bcv - T; }
-          else if (side[j] < 0) { acv = acv - 0.0; an[j] = an[j] - 0.0; bcv = bcv + T; }
+          if (SIDE(j) == 1u) { acv = acv + 0.0; an[j] = an[j] + 0.0; bcv = bcv - T; }
+          else if (SIDE(j) == 2u) { acv = acv - 0.0; an[j] = an[j] - 0.0; bcv = bcv + T; }
           else { acv = acv + 0.0; bcv = bcv - T; }
         }
 #pragma unroll
       for (int j = 0; j < kCellFaces; ++j)
-        if (j < nf && side[j] != 0) anb[r0 + j] = an[j];
+        if (j < nf && SIDE(j) != 0u) anb[r0 + j] = an[j];
+#undef SIDE
     } else {
       // (1) convection, sign +1
       for (int q = s; q < ne; ++q) {

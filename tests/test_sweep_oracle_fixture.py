@@ -70,3 +70,26 @@ def test_smallest_plain_sample_case_reproduces(oracle_mod):
     c = min(d["cases"], key=lambda c: c["first"]["6"] * c["cells"])
     first, _ = _rerun(c, 6, {"p_smoother": "MCGS"})
     assert first[6] == c["first"]["6"]
+
+
+def test_bench_error_vs_oracle_reads_the_fixture():
+    """bench.py's error_vs_oracle on fields whose distances are known: the oracle's own 1e-6
+    fields (where the fixture holds them) are as far from the fixed point as the fixture says,
+    and at distance zero from themselves under the same rule."""
+    import importlib.util
+    import types
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("ufvm_bench", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    z = np.load(os.path.join(GOLDEN, "sweep_oracle_fields.npz"))
+    pinned = [c for c in bench.oracle_pinned(0) if f"U_6_{c['index']}" in z.files]
+    assert len(pinned) >= 8
+    specs = {c["index"]: types.SimpleNamespace(mesh=types.SimpleNamespace(n_cells=c["cells"])) for c in pinned}
+    kept = {c["index"]: (z[f"U_6_{c['index']}"].astype(np.float64).reshape(-1),
+                         z[f"p_6_{c['index']}"].astype(np.float64)) for c in pinned}
+    out = bench.error_vs_oracle(pinned, specs, kept)
+    assert out["cases"] == len(pinned) and out["same_rule"]["u_max"] == 0.0 and out["same_rule"]["p_max"] == 0.0
+    # the stored 1e-6 fields are float32: their distance matches the fixture's FP64 one to rounding
+    assert 0.999 < out["u_over_oracle_own"]["min"] <= out["u_over_oracle_own"]["max"] < 1.001
+    assert 0.99 < out["p_over_oracle_own"]["min"] <= out["p_over_oracle_own"]["max"] < 1.01
