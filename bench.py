@@ -354,12 +354,12 @@ def tail_profile(tick_log, cases):
 ROOF_KERNEL = (1, "k_mc32_l0 (FP32 multicolour Gauss-Seidel sweep of the V-cycle's level 0, "
                   "colour-permuted ELL; one unit = both colours forward then backward over every case)")
 
-# DRAM traffic per byte of the bytes model, from one ncu capture of each unit's kernels on a
-# 160-case batch (profiles/k_uface_k_assemble_u_cavity_batch.md: k_uface + k_assemble_u moved
-# 1534.5 MB against 341.9 MB of the model; profiles/k_mc32_level0_cavity_sweep.md: 176.4 MB
-# against 188.3 MB). Traffic grows in proportion to the batch, so the live unit's traffic is
-# this ratio times its model bytes.
-TRAFFIC_PER_MODEL_BYTE = {3: 1534.5 / 341.9, 1: 176.4 / 188.3}
+# DRAM traffic per byte of the bytes model, from ncu captures of each unit's kernels on a
+# 160-case batch (profiles/k_uface_int_bnd_k_assemble_u_cavity_batch.md: k_uface_int + 3 x
+# (k_uface_bnd + k_assemble_u) moved 3922.4 MB against 1025.7 MB of the model;
+# profiles/k_mc32_level0_cavity_sweep.md: 176.4 MB against 188.3 MB). Traffic grows in
+# proportion to the batch, so the live unit's traffic is this ratio times its model bytes.
+TRAFFIC_PER_MODEL_BYTE = {3: 3922.4 / 1025.7, 1: 176.4 / 188.3}
 
 # Units of the service's profiling hook: (id, name, units per tick as a function of the tick's U
 # smoother sweeps and p V-cycles, bound)

@@ -383,9 +383,16 @@ __global__ void k_set_active(SolveCtl* ctl, int ns) {
 }
 
 // ---------------------------------------------------------------- FP32 AMG kernels
-// Galerkin by summation from level l into level l+1 (assembleAgglomeratedLHS.m:16-30 order)
-__global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
-                             const SolveCtl* __restrict__ ctl) {
+// Galerkin by summation from level l into level l+1 (assembleAgglomeratedLHS.m:16-30 order).
+// One thread per coarse row. A row of at most kGalW entries is accumulated in shared memory
+// (thread t's entry k at [k * kBlock + t]) and written once at the end; a wider row is
+// accumulated in place in global memory. Either way each coarse entry starts at 0.0 and takes
+// its fine entries in the same order: same bits.
+constexpr int kGalW = 16;
+__global__ void __launch_bounds__(kBlock) k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l,
+                                                       const int2* __restrict__ work,
+                                                       const SolveCtl* __restrict__ ctl) {
+  __shared__ double acc[kGalW * kBlock];
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& F = LEV(l, w.x);
@@ -393,6 +400,24 @@ __global__ void k_galerkin_b(const LevDesc* __restrict__ levTab, int ns, int l, 
   const int P = w.y * blockDim.x + threadIdx.x;
   if (P >= C.n) return;
   const int c0 = C.rowptr[P], c1 = C.rowptr[P + 1];
+  if (c1 - c0 <= kGalW && F.gpos) {
+    double* a = acc + threadIdx.x;
+    for (int t = 0; t < c1 - c0; ++t) a[t * kBlock] = 0.0;
+    double AC = 0.0;
+    for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) {
+      const int c = F.child[q];
+      AC = AC + F.ac64[c];
+      for (int k = F.rowptr[c]; k < F.rowptr[c + 1]; ++k) {
+        const int pos = F.gpos[k];  // -1 inside the aggregate, else the coarse entry
+        const double v = F.anb64[k];
+        if (pos == -1) AC = AC + v;
+        else if (pos >= 0) a[(pos - c0) * kBlock] = a[(pos - c0) * kBlock] + v;
+      }
+    }
+    for (int t = 0; t < c1 - c0; ++t) C.anb64[c0 + t] = a[t * kBlock];
+    C.ac64[P] = AC;
+    return;
+  }
   for (int t = c0; t < c1; ++t) C.anb64[t] = 0.0;
   double AC = 0.0;
   for (int q = F.childStart[P]; q < F.childStart[P + 1]; ++q) {
