@@ -22,6 +22,7 @@
 #include <atomic>
 #include <chrono>
 #include <thread>
+#include <utility>
 
 #include "fast.cuh"
 
@@ -260,10 +261,22 @@ __global__ void k_mc64(const SlotDesc* __restrict__ slots, const LevDesc* __rest
 
 // One colour of the FP64 U Gauss-Seidel from self-contained work items (the ELL copy of the
 // momentum matrix; same row arithmetic as k_mc64).
+// The colour kernels of a sweep are chained as programmatic dependent launches (every colour
+// launch but a sweep's first, see `launch_colour`): a kernel may start while the colour before it
+// runs. It loads what no colour kernel writes (its item, the active flag, the row's entries, bc
+// and ac) and then waits (griddepcontrol.wait: the previous kernel has completed and its writes
+// are visible) before it gathers x. Every thread waits, also one with no row, so that no colour
+// kernel completes before the one it follows; the kernel after a sweep is launched the ordinary
+// way and so starts after all of them. A launch without the attribute passes the wait at once;
+// the two give the same bits.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __global__ void k_mc64_items(const U0Item* __restrict__ items, const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();
   const U0Item& it = items[blockIdx.x];
   const int t = threadIdx.x;
-  if (t >= it.cnt || !ctl[it.slot].active) return;
+  if (t >= it.cnt || !ctl[it.slot].active) return pdl_wait();
   const int p = it.p0 + t;
   const size_t n = (size_t)it.n;
   const int W = it.W;
@@ -276,6 +289,7 @@ __global__ void k_mc64_items(const U0Item* __restrict__ items, const SolveCtl* _
   }
   double v = it.bc[p];
   const double d = it.ac[p];
+  pdl_wait();
   double xv[kEllUnroll];
 #pragma unroll
   for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? it.x[c[k]] : 0.0;
@@ -557,9 +571,10 @@ __device__ __forceinline__ void prolong_row32(const LevDesc& F, const LevDesc& C
 // the row range and the level's array pointers, so the only loads before the row data are the
 // item and the case's active flag (issued together).
 __global__ void k_mc32_l0(const L0Item* __restrict__ items, const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();
   const L0Item& it = items[blockIdx.x];
   const int t = threadIdx.x;
-  if (t >= it.cnt || !ctl[it.slot].active) return;
+  if (t >= it.cnt || !ctl[it.slot].active) return pdl_wait();
   const int p = it.p0 + t;
   const size_t n = (size_t)it.n;
   const int W = it.W;
@@ -572,6 +587,7 @@ __global__ void k_mc32_l0(const L0Item* __restrict__ items, const SolveCtl* __re
   }
   float v = it.bc[p];
   const float d = it.ac[p];
+  pdl_wait();
   float xv[kEllUnroll];
 #pragma unroll
   for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? it.x[c[k]] : 0.0f;
@@ -581,16 +597,43 @@ __global__ void k_mc32_l0(const L0Item* __restrict__ items, const SolveCtl* __re
   it.x[p] = v / d;
 }
 
-// One colour of a Gauss-Seidel sweep.
+// One colour of a Gauss-Seidel sweep (a grid level), chained like k_mc32_l0.
 __global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work, int color,
                        const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();
   const int2 w = work[blockIdx.x];
-  if (!ctl[w.x].active) return;
+  if (!ctl[w.x].active) return pdl_wait();
   const LevDesc& A = LEV(l, w.x);
-  if (color >= A.ncolor) return;
+  if (color >= A.ncolor) return pdl_wait();
   const int t = w.y * blockDim.x + threadIdx.x;
-  if (t >= A.colorStart[color + 1] - A.colorStart[color]) return;
-  gs_row32(A, color_row(A, color, t));
+  if (t >= A.colorStart[color + 1] - A.colorStart[color]) return pdl_wait();
+  const int p = color_row(A, color, t);
+  if (!A.pmode || A.ellW > kEllUnroll) {
+    pdl_wait();
+    gs_row32(A, p);
+    return;
+  }
+  // gs_row32 / row_sum32 on an ELL row of at most kEllUnroll entries, with the loads that do not
+  // read x before the wait: the same operations in the same order
+  const int W = A.ellW;
+  const size_t n = (size_t)A.n;
+  int c[kEllUnroll];
+  float a[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) {
+    c[k] = k < W ? A.ellCol[k * n + p] : -1;
+    a[k] = k < W ? A.ellAnb[k * n + p] : 0.0f;
+  }
+  float v = A.bc[p];
+  const float d = A.ac[p];
+  pdl_wait();
+  float xv[kEllUnroll];
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k) xv[k] = c[k] >= 0 ? A.x[c[k]] : 0.0f;
+#pragma unroll
+  for (int k = 0; k < kEllUnroll; ++k)
+    if (c[k] >= 0) v = v - a[k] * xv[k];
+  A.x[p] = v / d;
 }
 
 __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
@@ -756,6 +799,24 @@ __device__ void coarse_apply(const LevDesc& A, const double* __restrict__ X, con
 // starts at colour C-1, which the forward pass has just updated from the same neighbour values
 // (rows of one colour are not coupled, and a row's update x = (b - sum anb x_nb) / a does not
 // read its own x), so that update would write the same bits again: every sweep below skips it.
+// Before the barrier that ends a colour, each thread asks L1 for what its first row of the next
+// colour reads apart from x (the ELL entries, bc, ac: none of them changes while the level is
+// smoothed), so that after the barrier only the neighbour gathers wait on memory.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+__device__ __forceinline__ void prefetch_row32(const LevDesc& A, int c, int t) {
+  if (!A.pmode || t >= A.colorStart[c + 1] - A.colorStart[c]) return;
+  const int p = A.colorStart[c] + t;
+  const size_t n = (size_t)A.n;
+  for (int k = 0; k < A.ellW; ++k) {
+    prefetch_l1(A.ellCol + k * n + p);
+    prefetch_l1(A.ellAnb + k * n + p);
+  }
+  prefetch_l1(A.bc + p);
+  prefetch_l1(A.ac + p);
+}
+
 template <class D>
 __device__ void smooth_dom(const LevDesc& A, int sweeps, const D& d) {
   for (int sw = 0; sw < sweeps; ++sw)
@@ -764,6 +825,12 @@ __device__ void smooth_dom(const LevDesc& A, int sweeps, const D& d) {
         const int c = pass == 0 ? q : A.ncolor - 1 - q;
         const int cnt = A.colorStart[c + 1] - A.colorStart[c];
         for (int t = d.tid; t < cnt; t += d.nth) gs_row32(A, color_row(A, c, t));
+        // the colour after this one: the next in this pass, or the first of the next pass
+        int cn = -1;
+        if (pass == 0) cn = q + 1 < A.ncolor ? q + 1 : (A.ncolor >= 2 ? A.ncolor - 2 : -1);
+        else if (q + 1 < A.ncolor) cn = A.ncolor - 2 - q;
+        else if (sw + 1 < sweeps) cn = 0;
+        if (cn >= 0) prefetch_row32(A, cn, d.tid);
         d.sync();
       }
 }
@@ -835,6 +902,25 @@ template <typename T>
 static int upload_vec(DArr<T>& d, const std::vector<T>& h, cudaStream_t st) {
   UFVM_CHECK(dalloc(d, std::max<size_t>(h.size(), 1)));
   if (!h.empty()) UFVM_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return UFVM_OK;
+}
+
+// A colour kernel of a sweep: a sweep's first colour waits for all earlier work the ordinary
+// way, the later ones are programmatic dependents of the colour before them (they may start
+// while it runs and wait on the device before reading x; kernels in k_mc32, k_mc32_l0 and
+// k_mc64_items).
+template <typename... Exp, typename... Act>
+static int launch_colour(bool chained, void (*kernel)(Exp...), int grid, cudaStream_t st, Act&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kBlock);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = chained ? 1 : 0;
+  UFVM_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
   return UFVM_OK;
 }
 
@@ -1369,12 +1455,19 @@ int Service::solve_u(bool g) {
                                 SCAL_U_R1, anyflag.p, 0, h, loopcnt.p, 0);
   UFVM_LAUNCH_CHECK();
   auto body = [&]() -> int {
+    bool chained = false;
     for (int pass = 0; pass < 2; ++pass)
       for (int q = pass; q < ucolors; ++q) {  // the backward pass skips the repeated colour
         const int c = pass == 0 ? q : ucolors - 1 - q;
         if (ucol_cnt[c] == 0) continue;
-        if (u_items) k_mc64_items<<<ucol_cnt[c], kBlock, 0, stream>>>(wu_items.p + ucol_off[c], uctl.p);
-        else k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
+        if (u_items) {
+          UFVM_CHECK(launch_colour(chained, k_mc64_items, ucol_cnt[c], stream,
+                                   (const U0Item*)(wu_items.p + ucol_off[c]), (const SolveCtl*)uctl.p));
+          chained = true;
+        } else {
+          k_mc64<<<ucol_cnt[c], kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wu_col.p + ucol_off[c], c, uctl.p);
+          chained = false;
+        }
       }
     if (ures_items) k_res64_items<<<nwc, kBlock, 0, stream>>>(wures_items.p, uctl.p, part.p);
     else k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
@@ -1424,15 +1517,22 @@ int Service::solve_p(bool g) {
   k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, pctl.p, 1, s.p_max_cycles, s.p_termination, 0,
                                 SCAL_P_R0, SCAL_P_R1, anyflag.p, 0, h, loopcnt.p, 1);
   UFVM_LAUNCH_CHECK();
-  auto smooth = [&](int l, int sweeps) {
+  auto smooth = [&](int l, int sweeps) -> int {
+    bool chained = false;
     for (int k = 0; k < sweeps; ++k)
       for (int pass = 0; pass < 2; ++pass)
         for (int q = pass; q < maxcol[l]; ++q) {  // the backward pass skips the repeated colour
           const int c = pass == 0 ? q : maxcol[l] - 1 - q;
           if (smcnt[l][c] == 0) continue;
-          if (l == 0 && l0_items) k_mc32_l0<<<smcnt[0][c], kBlock, 0, stream>>>(wsm0.p + smoff[0][c], pctl.p);
-          else k_mc32<<<smcnt[l][c], kBlock, 0, stream>>>(levTab.p, ns, l, wsm[l].p + smoff[l][c], c, pctl.p);
+          if (l == 0 && l0_items)
+            UFVM_CHECK(launch_colour(chained, k_mc32_l0, smcnt[0][c], stream,
+                                     (const L0Item*)(wsm0.p + smoff[0][c]), (const SolveCtl*)pctl.p));
+          else
+            UFVM_CHECK(launch_colour(chained, k_mc32, smcnt[l][c], stream, (const LevDesc*)levTab.p, ns, l,
+                                     (const int2*)(wsm[l].p + smoff[l][c]), c, (const SolveCtl*)pctl.p));
+          chained = true;
         }
+    return UFVM_OK;
   };
   // flexible-CG scratch: (z, q_old) partials and sums, ((p, q), (p, r)) partials and sums
   const size_t o_zs = ((size_t)nwc + 1) & ~(size_t)1, o_pp = (o_zs + ns + 1) & ~(size_t)1,
@@ -1444,7 +1544,7 @@ int Service::solve_p(bool g) {
   auto cycle = [&]() -> int {
     // large levels as grid-wide launches, the small ones per slot in one CTA
     for (int l = 0; l < maxg; ++l) {
-      smooth(l, s.p_pre_sweep);
+      UFVM_CHECK(smooth(l, s.p_pre_sweep));
       k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
       k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
     }
@@ -1457,7 +1557,7 @@ int Service::solve_p(bool g) {
     }
     for (int l = maxg - 1; l >= 0; --l) {
       k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
-      smooth(l, s.p_post_sweep);
+      UFVM_CHECK(smooth(l, s.p_post_sweep));
     }
     if (s.p_krylov) {
       k_fcg_zq<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_part);
