@@ -135,6 +135,14 @@ int dalloc(DArr<T>& a, size_t n) {
   return UFVM_OK;
 }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialization may
+// start once every block of the kernel before it has executed pdl_trigger; pdl_wait then blocks
+// until that kernel has completed and its writes are visible. Without the launch attribute both
+// are no-ops. A kernel that waits before touching memory any earlier kernel writes behaves as
+// an ordinary launch, minus the launch gap.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---- block reductions (fixed shape => deterministic) ----
 __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -69,6 +69,8 @@ __device__ __forceinline__ double urow_sum(const LevDesc& A, int p, double v) {
 
 __global__ void k_res64_abs(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                             const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double* part) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int2 w = work[blockIdx.x];
   const SlotDesc& S = slots[w.x];
@@ -118,6 +120,8 @@ __global__ void k_u_from_ell(const SlotDesc* __restrict__ slots, const LevDesc* 
 // r = b - A x (FP64) -> FP32 right-hand side of the correction; e = 0
 __global__ void k_res64_rhs(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                             const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double* part) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int2 w = work[blockIdx.x];
   const SlotDesc& S = slots[w.x];
@@ -140,6 +144,8 @@ __global__ void k_res64_rhs(const SlotDesc* __restrict__ slots, const LevDesc* _
 
 __global__ void k_update64(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                            const int2* __restrict__ work, const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const SlotDesc& S = slots[w.x];
@@ -159,6 +165,8 @@ __global__ void k_update64(const SlotDesc* __restrict__ slots, const LevDesc* __
 // summed per slot in a fixed order.
 __global__ void k_fcg_zq(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                          const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double* part) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int2 w = work[blockIdx.x];
   const SlotDesc& S = slots[w.x];
@@ -173,6 +181,8 @@ __global__ void k_fcg_zq(const SlotDesc* __restrict__ slots, const LevDesc* __re
 __global__ void k_fcg_p(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                         const int2* __restrict__ work, const SolveCtl* __restrict__ ctl,
                         const double* __restrict__ zq, const double2* __restrict__ pqr) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const int2 w = work[blockIdx.x];
   const SolveCtl c = ctl[w.x];
   if (!c.active) return;
@@ -192,6 +202,8 @@ __global__ void k_fcg_p(const SlotDesc* __restrict__ slots, const LevDesc* __res
 
 __global__ void k_fcg_q(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                         const int2* __restrict__ work, const SolveCtl* __restrict__ ctl, double2* part) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int2 w = work[blockIdx.x];
   const SlotDesc& S = slots[w.x];
@@ -215,6 +227,8 @@ __global__ void k_fcg_q(const SlotDesc* __restrict__ slots, const LevDesc* __res
 __global__ void k_fcg_update(const SlotDesc* __restrict__ slots, const LevDesc* __restrict__ levTab, int ns,
                              const int2* __restrict__ work, const SolveCtl* __restrict__ ctl,
                              const double2* __restrict__ pqr, double* part) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int2 w = work[blockIdx.x];
   const SlotDesc& S = slots[w.x];
@@ -269,8 +283,6 @@ __global__ void k_mc64(const SlotDesc* __restrict__ slots, const LevDesc* __rest
 // kernel completes before the one it follows; the kernel after a sweep is launched the ordinary
 // way and so starts after all of them. A launch without the attribute passes the wait at once;
 // the two give the same bits.
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __global__ void k_mc64_items(const U0Item* __restrict__ items, const SolveCtl* __restrict__ ctl) {
   pdl_trigger();
@@ -302,6 +314,8 @@ __global__ void k_mc64_items(const U0Item* __restrict__ items, const SolveCtl* _
 // sum |r| block partials of the U system from self-contained items (wc order; the same row
 // values and block sums as k_res64_abs on the ELL copy)
 __global__ void k_res64_items(const U0Item* __restrict__ items, const SolveCtl* __restrict__ ctl, double* part) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const U0Item& it = items[blockIdx.x];
   const int t = threadIdx.x;
@@ -333,6 +347,8 @@ __global__ void k_res64_items(const U0Item* __restrict__ items, const SolveCtl* 
 // per-slot sums of block partials (fixed order)
 __global__ void k_slot_sum(const int* __restrict__ ws, const int* __restrict__ we, const double* __restrict__ part,
                            double* out) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int s = blockIdx.x;
   double v = 0.0;
@@ -343,6 +359,8 @@ __global__ void k_slot_sum(const int* __restrict__ ws, const int* __restrict__ w
 
 __global__ void k_slot_sum2(const int* __restrict__ ws, const int* __restrict__ we,
                             const double2* __restrict__ part, double2* out) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ double sh[32];
   const int s = blockIdx.x;
   double a = 0.0, b = 0.0;
@@ -358,6 +376,8 @@ __global__ void k_slot_sum2(const int* __restrict__ ws, const int* __restrict__ 
 __global__ void k_ctrl(const SlotDesc* __restrict__ slots, int ns, const double* __restrict__ sums, SolveCtl* ctl,
                        int first, int max_iter, double rrf, int divide_n, int r0_slot, int r1_slot, int* any,
                        int set_cond, cudaGraphConditionalHandle cond, unsigned long long* loops, int which) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   __shared__ int sany;
   if (threadIdx.x == 0) sany = 0;
   __syncthreads();
@@ -638,6 +658,8 @@ __global__ void k_mc32(const LevDesc* __restrict__ levTab, int ns, int l, const 
 
 __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
                         const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& A = LEV(l, w.x);
@@ -647,6 +669,8 @@ __global__ void k_res32(const LevDesc* __restrict__ levTab, int ns, int l, const
 
 __global__ void k_restrict32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
                              const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& F = LEV(l, w.x);
@@ -657,6 +681,8 @@ __global__ void k_restrict32(const LevDesc* __restrict__ levTab, int ns, int l, 
 
 __global__ void k_prolong32(const LevDesc* __restrict__ levTab, int ns, int l, const int2* __restrict__ work,
                             const SolveCtl* __restrict__ ctl) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const int2 w = work[blockIdx.x];
   if (!ctl[w.x].active) return;
   const LevDesc& F = LEV(l, w.x);
@@ -866,6 +892,8 @@ __global__ void __launch_bounds__(1024, 2) k_coarse_vcycle(const LevDesc* __rest
                                                         const int* __restrict__ gstart, const double* __restrict__ cinv,
                                                         int pre, int post, const SolveCtl* __restrict__ ctl,
                                                         const int* __restrict__ order) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const int s = order[blockIdx.x];
   if (!ctl[s].active) return;
   vcycle_levels(levTab, ns, s, coarsest[s], gstart[s], cinv, pre, post,
@@ -881,6 +909,8 @@ __global__ void __launch_bounds__(kBlockPack, 1) k_coarse_vcycle_pk(const LevDes
                                                                    const double* __restrict__ cinv, int pre, int post,
                                                                    const SolveCtl* __restrict__ ctl,
                                                                    const PackTask* __restrict__ tasks) {
+  pdl_trigger();  // a chained launch of the solve loops (see launch_k): start early, then
+  pdl_wait();     // wait for the kernel before it
   const PackTask& T = tasks[blockIdx.x];
   // one code path for both: a large slot is one group of the whole CTA on barrier 1
   const int gsize = T.big ? kBlockPack : kBlockPack / kPackGroups;
@@ -905,15 +935,20 @@ static int upload_vec(DArr<T>& d, const std::vector<T>& h, cudaStream_t st) {
   return UFVM_OK;
 }
 
-// A colour kernel of a sweep: a sweep's first colour waits for all earlier work the ordinary
-// way, the later ones are programmatic dependents of the colour before them (they may start
-// while it runs and wait on the device before reading x; kernels in k_mc32, k_mc32_l0 and
-// k_mc64_items).
+// Launches inside the solve loops' bodies. A chained launch is a programmatic dependent of the
+// kernel before it: it may start while that kernel runs and waits on the device (pdl_wait)
+// before it touches what earlier kernels wrote. The kernels launched this way wait at their top,
+// except the colour kernels (k_mc32, k_mc32_l0, k_mc64_items), which first load what no colour
+// kernel writes; so a sweep's first colour is never chained (its right-hand side may come from
+// the kernel just before it), and a body's first launch is never chained (it has no kernel
+// before it in the body's graph).
 template <typename... Exp, typename... Act>
-static int launch_colour(bool chained, void (*kernel)(Exp...), int grid, cudaStream_t st, Act&&... args) {
+static int launch_k(bool chained, void (*kernel)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                    Act&&... args) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kBlock);
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -922,6 +957,10 @@ static int launch_colour(bool chained, void (*kernel)(Exp...), int grid, cudaStr
   cfg.numAttrs = chained ? 1 : 0;
   UFVM_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
   return UFVM_OK;
+}
+template <typename... Exp, typename... Act>
+static int launch_colour(bool chained, void (*kernel)(Exp...), int grid, cudaStream_t st, Act&&... args) {
+  return launch_k(chained, kernel, dim3(grid), dim3(kBlock), 0, st, std::forward<Act>(args)...);
 }
 
 // blocks of n items for every slot passing `use`, with per-slot entry ranges
@@ -1469,12 +1508,15 @@ int Service::solve_u(bool g) {
           chained = false;
         }
       }
-    if (ures_items) k_res64_items<<<nwc, kBlock, 0, stream>>>(wures_items.p, uctl.p, part.p);
-    else k_res64_abs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, uctl.p, part.p);
-    k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
-    k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, uctl.p, 0, s.u_n_iter, s.u_rrf, 1, SCAL_U_R0,
-                                  SCAL_U_R1, anyflag.p, g, h, loopcnt.p, 0);
-    UFVM_LAUNCH_CHECK();
+    if (ures_items)
+      UFVM_CHECK(launch_k(chained, k_res64_items, dim3(nwc), dim3(kBlock), 0, stream, wures_items.p, uctl.p, part.p));
+    else
+      UFVM_CHECK(launch_k(chained, k_res64_abs, dim3(nwc), dim3(kBlock), 0, stream, slotTab.p, levTab.p, ns, wc.p,
+                          uctl.p, part.p));
+    UFVM_CHECK(launch_k(true, k_slot_sum, dim3(ns), dim3(256), 0, stream, cstart.p, cend.p, part.p,
+                        part.p + nwc + 8));
+    UFVM_CHECK(launch_k(true, k_ctrl, dim3(1), dim3(256), 0, stream, slotTab.p, ns, part.p + nwc + 8, uctl.p, 0,
+                        s.u_n_iter, s.u_rrf, 1, SCAL_U_R0, SCAL_U_R1, anyflag.p, g, h, loopcnt.p, 0));
     return UFVM_OK;
   };
   if (g) {
@@ -1542,38 +1584,44 @@ int Service::solve_p(bool g) {
   double2* pqr_part = reinterpret_cast<double2*>(fcg.p + o_pp);
   double2* pqr_sum = reinterpret_cast<double2*>(fcg.p + o_ps);
   auto cycle = [&]() -> int {
-    // large levels as grid-wide launches, the small ones per slot in one CTA
+    // large levels as grid-wide launches, the small ones per slot in one CTA; every launch after
+    // the body's first kernel is chained except a sweep's first colour
+    const dim3 B(kBlock);
     for (int l = 0; l < maxg; ++l) {
       UFVM_CHECK(smooth(l, s.p_pre_sweep));
-      k_res32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
-      k_restrict32<<<nwrc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wrc[l].p, pctl.p);
+      UFVM_CHECK(launch_k(true, k_res32, dim3(nwnc[l]), B, 0, stream, levTab.p, ns, l, wnc[l].p, pctl.p));
+      UFVM_CHECK(launch_k(true, k_restrict32, dim3(nwrc[l]), B, 0, stream, levTab.p, ns, l, wrc[l].p, pctl.p));
     }
+    const bool after = maxg > 0;  // a kernel of this body came before
     if (use_packing && npk_tasks > 0) {
-      k_coarse_vcycle_pk<<<npk_tasks, kBlockPack, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p,
-                                                              s.p_pre_sweep, s.p_post_sweep, pctl.p, dpk_tasks.p);
+      UFVM_CHECK(launch_k(after, k_coarse_vcycle_pk, dim3(npk_tasks), dim3(kBlockPack), 0, stream, levTab.p, ns,
+                          dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep, s.p_post_sweep, pctl.p, dpk_tasks.p));
     } else {
-      k_coarse_vcycle<<<ns, 1024, 0, stream>>>(levTab.p, ns, dcoarsest.p, dgstart.p, cinv.p, s.p_pre_sweep,
-                                               s.p_post_sweep, pctl.p, dcta_order.p);
+      UFVM_CHECK(launch_k(after, k_coarse_vcycle, dim3(ns), dim3(1024), 0, stream, levTab.p, ns, dcoarsest.p,
+                          dgstart.p, cinv.p, s.p_pre_sweep, s.p_post_sweep, pctl.p, dcta_order.p));
     }
     for (int l = maxg - 1; l >= 0; --l) {
-      k_prolong32<<<nwnc[l], kBlock, 0, stream>>>(levTab.p, ns, l, wnc[l].p, pctl.p);
+      UFVM_CHECK(launch_k(true, k_prolong32, dim3(nwnc[l]), B, 0, stream, levTab.p, ns, l, wnc[l].p, pctl.p));
       UFVM_CHECK(smooth(l, s.p_post_sweep));
     }
     if (s.p_krylov) {
-      k_fcg_zq<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_part);
-      k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, zq_part, zq_sum);
-      k_fcg_p<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_sum, pqr_sum);
-      k_fcg_q<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, pqr_part);
-      k_slot_sum2<<<ns, 256, 0, stream>>>(cstart.p, cend.p, pqr_part, pqr_sum);
-      k_fcg_update<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, pqr_sum, part.p);
+      UFVM_CHECK(launch_k(true, k_fcg_zq, dim3(nwc), B, 0, stream, slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_part));
+      UFVM_CHECK(launch_k(true, k_slot_sum, dim3(ns), dim3(256), 0, stream, cstart.p, cend.p, zq_part, zq_sum));
+      UFVM_CHECK(launch_k(true, k_fcg_p, dim3(nwc), B, 0, stream, slotTab.p, levTab.p, ns, wc.p, pctl.p, zq_sum,
+                          pqr_sum));
+      UFVM_CHECK(launch_k(true, k_fcg_q, dim3(nwc), B, 0, stream, slotTab.p, levTab.p, ns, wc.p, pctl.p, pqr_part));
+      UFVM_CHECK(launch_k(true, k_slot_sum2, dim3(ns), dim3(256), 0, stream, cstart.p, cend.p, pqr_part, pqr_sum));
+      UFVM_CHECK(launch_k(true, k_fcg_update, dim3(nwc), B, 0, stream, slotTab.p, levTab.p, ns, wc.p, pctl.p,
+                          pqr_sum, part.p));
     } else {
-      k_update64<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p);
-      k_res64_rhs<<<nwc, kBlock, 0, stream>>>(slotTab.p, levTab.p, ns, wc.p, pctl.p, part.p);
+      UFVM_CHECK(launch_k(true, k_update64, dim3(nwc), B, 0, stream, slotTab.p, levTab.p, ns, wc.p, pctl.p));
+      UFVM_CHECK(launch_k(true, k_res64_rhs, dim3(nwc), B, 0, stream, slotTab.p, levTab.p, ns, wc.p, pctl.p,
+                          part.p));
     }
-    k_slot_sum<<<ns, 256, 0, stream>>>(cstart.p, cend.p, part.p, part.p + nwc + 8);
-    k_ctrl<<<1, 256, 0, stream>>>(slotTab.p, ns, part.p + nwc + 8, pctl.p, 0, s.p_max_cycles, s.p_termination, 0,
-                                  SCAL_P_R0, SCAL_P_R1, anyflag.p, g, h, loopcnt.p, 1);
-    UFVM_LAUNCH_CHECK();
+    UFVM_CHECK(launch_k(true, k_slot_sum, dim3(ns), dim3(256), 0, stream, cstart.p, cend.p, part.p,
+                        part.p + nwc + 8));
+    UFVM_CHECK(launch_k(true, k_ctrl, dim3(1), dim3(256), 0, stream, slotTab.p, ns, part.p + nwc + 8, pctl.p, 0,
+                        s.p_max_cycles, s.p_termination, 0, SCAL_P_R0, SCAL_P_R1, anyflag.p, g, h, loopcnt.p, 1));
     return UFVM_OK;
   };
   if (g) {
