@@ -735,13 +735,26 @@ __global__ void __launch_bounds__(1024) k_coarse_factor(const LevDesc* __restric
   if (threadIdx.x == 0) s_scale = scale;
   __syncthreads();
   for (int k = 0; k < n; ++k) {
-    if (threadIdx.x == 0) {
-      int p = k;
-      double best = fabs(sm.M[k][k]);
-      for (int i = k + 1; i < n; ++i)
-        if (fabs(sm.M[i][k]) > best) { best = fabs(sm.M[i][k]); p = i; }
-      sm.piv_row = p;
-      if (best <= 1e-9 * s_scale) sm.pinned[k] = 1;
+    if (threadIdx.x < 32) {
+      // partial pivoting: the first row of the largest |M[i][k]|, i >= k (each lane takes rows
+      // k + lane, k + lane + 32, ... in order, then the lanes' bests are merged preferring the
+      // lower row on equal values: the row a sequential search would pick)
+      const int lane = threadIdx.x;
+      int p = -1;
+      double best = 0.0;
+      for (int i = k + lane; i < n; i += 32) {
+        const double v = fabs(sm.M[i][k]);
+        if (p < 0 || v > best) { best = v; p = i; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int op = __shfl_down_sync(0xffffffffu, p, o);
+        if (op >= 0 && (p < 0 || ob > best || (ob == best && op < p))) { best = ob; p = op; }
+      }
+      if (lane == 0) {
+        sm.piv_row = p;
+        if (best <= 1e-9 * s_scale) sm.pinned[k] = 1;
+      }
     }
     __syncthreads();
     if (sm.pinned[k]) continue;  // uniform across the block

@@ -14,9 +14,9 @@
 // are admitted, when the device time spent on them since they froze (their share of each tick, by
 // cells) reaches the host time the last drop and rebuild took, when one has waited
 // kMaxFrozenSteps steps, or when no active case is left. A departed case's device memory is
-// freed later, when admission finds too little free memory or the service ends: cudaFree waits
-// for the whole device, and freeing every case at its departure cost more host time than the
-// rest of the departures together.
+// freed later, when admission finds too little free memory or the service ends. The service's
+// arrays are stream-ordered allocations (common.cuh), so a free no longer waits for the device,
+// but a departed case's hundreds of frees still stay out of the steps that run the batch.
 #include <deque>
 #include <map>
 #include <memory>
@@ -80,9 +80,9 @@ struct ServiceImpl {
   // tables with its graph capture, plus freeing the departed cases)
   double waste_ms = 0.0, last_drop_ms = 0.0, host_drop_ms = 0.0;
   double host_admit_ms = 0.0;  // host time in admissions
-  // Cases that left the batch are not freed at once: freeing a case's device arrays
-  // (cudaFree, which waits for the whole device) costs far more host time than the rest of a
-  // departure. They wait here until admission finds too little memory, or the service ends.
+  // Cases that left the batch are not freed at once: freeing a case's device arrays (hundreds
+  // of them) costs more host time than the rest of a departure. They wait here until admission
+  // finds too little memory, or the service ends.
   std::vector<Case*> graveyard;
   void bury() {
     if (graveyard.empty()) return;
