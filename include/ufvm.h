@@ -174,8 +174,8 @@ int ufvm_solve_sor(int32_t n, const int32_t* rowptr, const int32_t* col, const d
  * clears what it needs; calls whose device work overlaps race on it and must be serialised.
  * The matrix must be structurally symmetric (every finite-volume matrix is), as for
  * ufvm_solve_sor: the level schedule is built from each row's lower neighbours.
- * The first call on a device looks the array up with cudaGetSymbolAddress: make it before any
- * stream capture. Results are bit-identical to ufvm_solve_sor's. */
+ * Every call synchronises its stream (it reads the level schedule's size back to the host), so
+ * it cannot be captured into a CUDA graph. Results are bit-identical to ufvm_solve_sor's. */
 int ufvm_solve_sor_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col, const double* ac,
                            const double* anb, const double* bc, double* dphi, void* stream);
 /* [dc] = cfdFactorizeILU and dphi = cfdSolveILU (solve/cfdFactorizeILU.m, cfdSolveILU.m). */

@@ -21,9 +21,10 @@
 //     finite-volume matrix is): the dependency levels come from each row's lower neighbours,
 //     which orders the sweep correctly only when a row's upper neighbours list it in turn;
 //     ufvm_solve_sor makes the same assumption;
-//   * the first call on a device looks up the scratch array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that first call
-//     before any stream capture that might include this function.
+//   * every call reads the level schedule's size back to the host and synchronises its stream
+//     (it builds the schedule on the device, then sizes the launches from it), so it cannot be
+//     captured into a CUDA graph; the first call on a device also looks up the scratch array's
+//     device address with cudaGetSymbolAddress (with that device current) and caches it.
 //
 // The sweep runs one kernel launch per dependency level (forward levels, then backward levels),
 // so every row sees exactly the neighbour values the sequential sweep would see, and each row
