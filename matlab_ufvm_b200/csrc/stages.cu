@@ -425,9 +425,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_uface_bnd(const SlotDesc* __restr
 
 constexpr int kCellFaces = 8;  // cells with at most this many faces take the register path
 
-// cfdAssembleEquation('U', comp): the face terms of k_uface scattered into the cell's row in
-// the reference's order -- convection over the cell's faces, the convection divergence,
-// diffusion, explicit stress -- then grad(p), false transient, URF, scaled residual, DU.
+// cfdAssembleEquation('U', comp): the staged face terms (k_uface_int, k_uface_bnd) added into
+// the cell's row in the reference's order -- convection over the cell's faces, the convection
+// divergence, diffusion, explicit stress -- then grad(p), false transient, URF, scaled
+// residual, DU.
 __global__ void __launch_bounds__(kBlock) k_assemble_u(const SlotDesc* __restrict__ slots,
                                                        const int2* __restrict__ work, int comp, double* part) {
   __shared__ double sh[32];
