@@ -140,8 +140,9 @@ struct Service {
   unsigned long long loops_seen[2] = {0, 0};
 
   // schedule: levels of at most cta_rows rows are smoothed inside the per-case CTA of the coarse
-  // V-cycle kernel, larger ones by grid-wide launches over all cases
-  int cta_rows = 8192;
+  // V-cycle kernel, larger ones by grid-wide launches over all cases (the autotuner's start: the
+  // threshold it kept on the cavity batches)
+  int cta_rows = 4096;
   // the coarse V-cycle packs small cases kPackGroups to a CTA (1) or runs one CTA per case (0);
   // a case with more than pk_rows rows below its grid levels gets a whole CTA
   int use_packing = 1;

@@ -110,12 +110,15 @@ struct ServiceImpl {
   long long steps_since_admit = 1 << 30;
   // schedule autotuner: times the candidate CTA thresholds of the V-cycle on the live batch
   // (graph-replayed steps only; the first step after each switch, which re-captures the graph,
-  // is not timed), interleaved over two rounds, and keeps the fastest. The threshold does not
-  // change any result, only which launches run the small levels. Re-tunes every tune_every steps.
+  // is not timed) over two rounds, the second in reverse order so that a batch whose ticks get
+  // shorter as cases finish favours no candidate, and switches to the fastest only if it beats
+  // the threshold in use by kTuneMargin. The threshold does not change any result, only which
+  // launches run the small levels. Re-tunes every tune_every steps.
   bool tune_on = true;
   long long tune_every = 2000, next_tune = 24, steps = 0;
   std::vector<int> tune_cand = {2048, 4096, 8192, 16384, 65536};
   int tune_pos = -1, tune_in_cand = 0;  // position in the candidate sequence; steps at it
+  int tune_prev = 0;                    // the threshold in use when the tuning started
   std::vector<double> tune_ms;
   std::vector<int> tune_n;
   std::vector<long long> finished_unpolled;  // tickets finished since the last poll
@@ -477,20 +480,24 @@ static bool snapshot(ServiceImpl& S, Record& r, Case& C) {
 }
 
 // One step of the schedule autotuner (called after every timed step).
+constexpr double kTuneMargin = 0.02;
 static void tune_step(ServiceImpl& S, double ms, bool graph_step) {
   if (!S.tune_on) return;
   const int nc = (int)S.tune_cand.size();
+  // candidate at sequence position q: forward in the first round, backward in the second
+  auto cand_at = [nc](int q) { return q < nc ? q : 2 * nc - 1 - q; };
   if (S.tune_pos < 0) {
     if (S.steps < S.next_tune || S.svc.cases.size() < 2) return;
     S.tune_ms.assign(nc, 0.0);
     S.tune_n.assign(nc, 0);
     S.tune_pos = 0;
     S.tune_in_cand = 0;
-    S.svc.cta_rows = S.tune_cand[0];
+    S.tune_prev = S.svc.cta_rows;
+    S.svc.cta_rows = S.tune_cand[cand_at(0)];
     S.svc.tables_dirty = true;
     return;
   }
-  const int cand = S.tune_pos % nc;
+  const int cand = cand_at(S.tune_pos);
   // step 0 at a candidate re-captures the graph; steps 1-2 are timed
   if (S.tune_in_cand >= 1 && graph_step) {
     S.tune_ms[cand] += ms;
@@ -499,17 +506,22 @@ static void tune_step(ServiceImpl& S, double ms, bool graph_step) {
   if (++S.tune_in_cand < 3) return;
   S.tune_in_cand = 0;
   if (++S.tune_pos < 2 * nc) {
-    S.svc.cta_rows = S.tune_cand[S.tune_pos % nc];
+    S.svc.cta_rows = S.tune_cand[cand_at(S.tune_pos)];
     S.svc.tables_dirty = true;
     return;
   }
-  int best = -1;
+  int best = -1, prev = -1;
   double best_ms = 0;
-  for (int k = 0; k < nc; ++k)
-    if (S.tune_n[k] > 0 && (best < 0 || S.tune_ms[k] / S.tune_n[k] < best_ms)) {
+  for (int k = 0; k < nc; ++k) {
+    if (S.tune_n[k] == 0) continue;
+    if (S.tune_cand[k] == S.tune_prev) prev = k;
+    if (best < 0 || S.tune_ms[k] / S.tune_n[k] < best_ms) {
       best = k;
       best_ms = S.tune_ms[k] / S.tune_n[k];
     }
+  }
+  // keep the threshold in use unless the fastest candidate is clearly faster
+  if (prev >= 0 && best_ms >= (1.0 - kTuneMargin) * (S.tune_ms[prev] / S.tune_n[prev])) best = prev;
   if (best >= 0) S.svc.cta_rows = S.tune_cand[best];
   S.svc.tables_dirty = true;
   S.tune_pos = -1;
