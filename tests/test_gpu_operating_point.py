@@ -24,8 +24,9 @@ residual near 1e-11 for 1e-6). Checked, per case:
   1e-6 stop (at most SAME_SIZE times it);
 * for n <= 128, the service's 1e-6 fields against the oracle's 1e-6 fields (the same stopping
   rule on both sides) differ by less than the sum of the two stops' errors;
-* at the tight stop, the service's field error is <= 1e-6 beyond the
-  oracle's own error at that stop: zero where the oracle's fixed point is its 1e-11 iterate;
+* at the tight stop, the service's field error is <= 1e-6 (the field tolerance of the batch
+  workload) beyond the oracle's own error at that stop: zero where the oracle's fixed point is
+  its 1e-11 iterate;
   2.0e-6 (U) and 1.0e-6 (p) for n=253 Re=121, whose residual stagnates before its fields reach
   1e-6 of the fixed point (the oracle's fields at 1e-10 are that far from its last iterate).
 """
