@@ -182,7 +182,8 @@ static bool device_room(size_t* room) {
 
 static long long estimate_raw(long long Nc, long long F, long long Fi, long long nodes) {
   const long long Fb = F - Fi, R = Nc + Fb, nnz = 2 * Fi;
-  const long long dbl = 19 * F + 4 * Nc + 23 * R + 10 * F + 8 * Nc + 2 * (nnz + 8 * Nc) + 4 * nnz;
+  // per face: 19 geometry arrays, mdot, two Rhie-Chow coefficients and 3 x 7 staged momentum terms
+  const long long dbl = 19 * F + 4 * Nc + 23 * R + 24 * F + 8 * Nc + 2 * (nnz + 8 * Nc) + 4 * nnz;
   const long long ints = 3 * F + 4 * Fi + 6 * Nc + 3 * nnz + nodes / 4;
   return 8 * dbl + 4 * ints;
 }
